@@ -1,0 +1,382 @@
+#!/usr/bin/env python
+"""Gibbs tokens/s per sweep of the EZLDA collapsed-Gibbs sweep on the K=1024 workload.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Workload (one "step" = one full sweep: word-topic + topic-total rebuild, per-word max
+topics, per-chunk doc-topic rebuild and sampling): a seeded synthetic corpus from the LDA
+generative process standing in for EZLDA's PubMed run (EZLDA/mainKernel.cu:56; the data
+are not available): D=300,000 docs, V=100,000 words, lognormal(5.3,0.6) doc lengths
+clipped to [20,2000] (~71.9M tokens), 256 generating topics, Zipf(1.05) word base measure,
+K=1024, alpha=50/K, beta=0.01, top-2% words dense, 8 chunks.  The K timed sweeps are
+sweeps 0..K-1 of training from the random initial topics (the warm-up sweeps run first and
+the topics are then reset), so the number is the average over a training run, early
+(dense doc rows, few early accepts) and late sweeps alike.
+
+--impl reference times the CPU restatement of the reference's sweep on the host cores.
+EZLDA has no CPU implementation of its sampler, so that arm runs the oracle port
+(oracle/liblda_oracle.c) with all host threads on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "gibbs_tokens_per_s_per_iter"
+UNIT = "tokens/s"
+WORKLOAD = ("lognormal K=1024 corpus: D=300000 V=100000 len~lognormal(5.3,0.6) in [20,2000] "
+            "(~71.9M tokens), 256 generating topics, Zipf(1.05) phi base, alpha=50/K, beta=0.01, "
+            "top-2% dense words, 8 chunks; sweeps 0..K-1 from random initial topics")
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-word-stride", type=int, default=40)
+    p.add_argument("--preset", default="c1")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except (OSError, ValueError):
+        return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the sampler from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "k_sample_c1_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms while running."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def physical_gpu(local: int) -> int:
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [x for x in vis.split(",") if x.strip()]
+        if local < len(ids) and ids[local].strip().isdigit():
+            return int(ids[local])
+    return local
+
+
+def make_corpus(preset: str, rank: int):
+    import lda_sc20_b200 as L
+    base = L.corpus_config(preset)
+    return L.Corpus.generate(L.corpus_config(preset, corpus_seed=base.corpus_seed + rank))
+
+
+def sampler_algorithmic_bytes(cnt, K: int, dense_words_per_sweep: int, sweeps: int, launches: int) -> float:
+    """Algorithmic bytes of the sampler over the timed region: per token 16 B (doc id, old
+    topic, new topic, doc length), 4 B per doc-row entry of every token whose S is evaluated,
+    4*K per dense word column and 4 B per sparse word-row entry (per chunk launch), 4*K for
+    n_k per launch."""
+    return (16.0 * cnt.tokens + 4.0 * cnt.sum_nnz_full + 4.0 * K * dense_words_per_sweep * sweeps
+            + 4.0 * cnt.sum_word_nnz + 4.0 * K * launches)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+    import lda_sc20_b200 as L
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    corpus = make_corpus(args.preset, rank)
+    info = corpus.info
+    K = info.K_hint
+    N = info.num_tokens
+    tr = L.Trainer(corpus, K=K, seed=42, device=local)
+    stream = torch.cuda.current_stream()
+    tr.set_stream(stream.cuda_stream)
+    z0 = corpus.topics()
+    seg = corpus.seg_cnt()
+    dense_words_per_sweep = int((seg[:, :info.num_dense] > 0).sum())
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def reduce_max(x: float) -> float:
+        if world == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    clocks = ClockSampler(physical_gpu(local))
+    clocks.start()
+    tr.iterate(args.warmup)                      # untimed warm-up sweeps
+    tr.set_topics(z0)                            # time sweeps 0..K-1 of a fresh run
+    tr.iteration = 0
+    tr.reset_stats()
+    tr.set_timing(True)
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tr.iterate(args.steps, ll=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    ms_local = e0.elapsed_time(e1)
+    ms = reduce_max(ms_local)
+    tm = tr.timing()
+    cnt = tr.counters()
+    tr.set_timing(False)
+    # log-likelihood of the state after the K timed sweeps (one extra evaluation sweep)
+    z_after = tr.topics()
+    ll_mean = tr.iterate(1, ll=True)
+    # sweep time with the FP64 LL evaluated every sweep (LL mode evaluates S for all tokens)
+    tr.set_topics(z0)
+    tr.iteration = 0
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    n_ll = max(1, min(args.steps, 10))
+    e2.record(stream)
+    tr.iterate(n_ll, ll=True)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_ll_sweep = e2.elapsed_time(e3) / n_ll
+
+    sweeps = args.steps
+    value = world * N * sweeps / (ms / 1e3)
+    launches_sample = tm.launches_sample
+    alg_bytes = sampler_algorithmic_bytes(cnt, K, dense_words_per_sweep, sweeps, launches_sample)
+    ms_per_launch = tm.ms_sample / max(launches_sample, 1)
+    achieved = alg_bytes / launches_sample / (ms_per_launch / 1e3) / 1e9 if launches_sample else None
+    peaks, peak_src = measured_peaks()
+    peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
+    traffic = ncu_traffic()
+
+    # end to end through the C ABI with pinned host buffers: upload topics, sweep, download
+    e2e = None
+    if not args.no_e2e:
+        zin = torch.from_numpy(z0.view(np.int16).copy()).pin_memory()
+        zout = torch.empty_like(zin).pin_memory()
+        tr.iteration = 0
+        tr.iterate_host(zin.numpy().view(np.uint16), zout.numpy().view(np.uint16))  # warm-up call
+        tr.iteration = 0
+        zin.copy_(torch.from_numpy(z0.view(np.int16)))
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        a, b = zin, zout
+        for _ in range(sweeps):
+            tr.iterate_host(a.numpy().view(np.uint16), b.numpy().view(np.uint16))
+            a, b = b, a
+        t1 = time.perf_counter()
+        barrier()
+        e2e_s = reduce_max(t1 - t0)
+        assert np.array_equal(a.numpy().view(np.uint16), z_after), "host-buffer sweeps diverged from resident sweeps"
+        e2e = {"value": world * N * sweeps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * N,
+               "d2h_bytes_per_step": 2 * N, "ms_per_step": 1e3 * e2e_s / sweeps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(corpus, tr, z0, K, sweeps, args.cpu_word_stride)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": sweeps,
+            "warmup": args.warmup, "ms_per_step": ms / sweeps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "tokens": N, "docs": info.num_docs, "vocab": info.vocab,
+                       "K": K, "dense_words": info.num_dense, "chunks": info.num_chunks,
+                       "l2": "inputs_larger_than_l2 (resident corpus ~1.6 GB per sweep pass)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "loglik_per_token": ll_mean,
+            "ms_per_step_with_ll": ms_ll_sweep,
+            "e2e": e2e,
+            "gpu_launches": tm.launches_wt + tm.launches_stats + tm.launches_dt + tm.launches_sample + tm.launches_ll,
+            "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                         "peak_source": f"{peak_src} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg_bytes / max(launches_sample, 1),
+                         "ms_per_launch": ms_per_launch},
+            "stages_ms_per_sweep": {"wt": tm.ms_wt / sweeps, "stats": tm.ms_stats / sweeps,
+                                    "dt": tm.ms_dt / sweeps, "sample": tm.ms_sample / sweeps},
+            "sweep_counters": {"early_accept_frac": cnt.early_accept / max(cnt.tokens, 1),
+                               "mean_nnz_full": cnt.sum_nnz_full / max(cnt.full, 1),
+                               "branch_max": cnt.branch_max, "branch_s": cnt.branch_s, "branch_q": cnt.branch_q},
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    tr.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def cpu_baseline(corpus, tr, z0, K, sweeps, stride):
+    """Oracle port on the host cores at the training state of sweep K/2 (a representative
+    mid-run state): full count rebuild plus sampling of every `stride`-th word."""
+    import numpy as np
+    from oracle import Oracle
+    tr.set_topics(z0)
+    tr.iteration = 0
+    tr.iterate(sweeps // 2)
+    zmid = tr.topics()
+    info = corpus.info
+    nt = os.cpu_count() or 1
+    o = Oracle(corpus.tok_word(), corpus.tok_doc(), info.vocab, info.num_docs, K, tr.alpha, tr.beta, nthreads=nt)
+    t0 = time.perf_counter()
+    o.rebuild(zmid)
+    t1 = time.perf_counter()
+    zz = zmid.copy()
+    st = o.sample(zz, 42, sweeps // 2, word_stride=stride)
+    t2 = time.perf_counter()
+    N = info.num_tokens
+    per_sweep = (t1 - t0) + (t2 - t1) * N / max(st.tokens, 1)
+    g = tr.topics()
+    sel = (corpus.tok_word() % stride) == 0
+    tr.set_topics(zmid)
+    tr.iteration = sweeps // 2
+    tr.iterate(1)
+    agree = bool(np.array_equal(tr.topics()[sel], zz[sel]))
+    del g
+    return {"value": N / per_sweep, "unit": UNIT, "cores": nt, "kind": "port",
+            "sample": (f"state after sweep {sweeps // 2}: full rebuild of all counts ({t1 - t0:.2f} s) + "
+                       f"sampling every {stride}th word ({st.tokens} of {N} tokens, {t2 - t1:.2f} s), "
+                       f"extrapolated to one sweep; GPU agrees token-for-token on the sample: {agree}")}
+
+
+def run_reference(args, world, rank, local):
+    """CPU restatement of the reference sweep (oracle port), all host threads."""
+    if rank != 0:
+        return
+    from oracle import Oracle
+    corpus = make_corpus(args.preset, 0)
+    info = corpus.info
+    K = info.K_hint
+    N = info.num_tokens
+    nt = os.cpu_count() or 1
+    alpha, beta = 50.0 / K, 0.01
+    o = Oracle(corpus.tok_word(), corpus.tok_doc(), info.vocab, info.num_docs, K, alpha, beta, nthreads=nt)
+    z = corpus.topics()
+    t0 = time.perf_counter()
+    o.rebuild(z)
+    t_rebuild = time.perf_counter() - t0
+    stride = max(1, args.cpu_word_stride * 10)
+    times, toks = [], 0
+    for s in range(args.warmup + args.steps):
+        zz = z.copy()
+        t1 = time.perf_counter()
+        st = o.sample(zz, 42, 0, word_stride=stride)
+        dt = time.perf_counter() - t1
+        if s >= args.warmup:
+            times.append(dt)
+            toks = st.tokens
+    per_sweep = t_rebuild + statistics.mean(times) * N / max(toks, 1)
+    value = N / per_sweep
+    sample = (f"sweep 0 state: full count rebuild ({t_rebuild:.2f} s, once) + per step sampling of every "
+              f"{stride}th word ({toks} of {N} tokens), extrapolated to one sweep; {nt} threads")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * per_sweep, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "tokens": N, "K": K}, "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,225 @@
+/*
+ * lda_b200.h -- C ABI of the B200-native collapsed-Gibbs LDA sweep.
+ *
+ * Drop-in boundary for EZLDA's hot path (asherliu/LDA_SC20).  EZLDA has no
+ * FFI: its boundary is (1) the C++ kernel-launch wrappers of its L2 layer
+ * (EZLDA/<stage>Kernel.cuh), called by the driver loop in EZLDA/mainKernel.cu, and
+ * (2) the on-disk chunk directory plus the K/alpha/beta/iteration parameters
+ * and the per-iteration log-likelihood line.  Every entry point below names the
+ * reference interface it replaces.  Conventions:
+ *   - plain pointers and sizes only; every function returns an int status
+ *     (LDA_OK = 0, negative on error) and never exits the process; the text of
+ *     the last error on the calling thread is in lda_last_error();
+ *   - host buffers are owned by the caller, device buffers by the library;
+ *   - one handle per host thread (handles are not internally locked);
+ *   - topics are 0-based here (the chunk files hold 1-based topics).
+ */
+#ifndef LDA_B200_H_
+#define LDA_B200_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LDA_OK 0
+#define LDA_ERR_ARG (-1)        /* bad argument or out-of-range value */
+#define LDA_ERR_IO (-2)         /* missing / unreadable / unwritable file */
+#define LDA_ERR_FORMAT (-3)     /* malformed or truncated chunk file */
+#define LDA_ERR_NOMEM (-4)      /* host allocation failed */
+#define LDA_ERR_DEVICE_MEM (-5) /* device memory budget or cudaMalloc exceeded */
+#define LDA_ERR_CUDA (-6)       /* CUDA runtime error (no device, launch failure, ...) */
+#define LDA_ERR_STATE (-7)      /* call not valid in the handle's current state */
+#define LDA_ERR_DEVICE (-8)     /* a kernel reported an out-of-range value */
+
+typedef struct lda_corpus lda_corpus;
+typedef struct lda_trainer lda_trainer;
+
+const char* lda_last_error(void);
+const char* lda_version(void);
+
+/* ------------------------------------------------------------------ corpus */
+
+/* Synthetic corpus drawn from the LDA generative process. */
+typedef struct {
+    int64_t num_docs;    /* D */
+    int64_t vocab;       /* V */
+    int32_t gen_topics;  /* generating topics */
+    int32_t len_kind;    /* 0: Poisson(len_p1); 1: lognormal(mu=len_p1, sigma=len_p2) */
+    double len_p1, len_p2;
+    int32_t len_min, len_max; /* clip */
+    int32_t phi_kind;    /* 0: phi_k ~ Dir(phi_conc * 1_V);
+                            1: phi_k ~ Dir(phi_conc * V * z), z_r ∝ (r+1)^-phi_zipf_s, sum z = 1 */
+    double phi_conc, phi_zipf_s;
+    double theta_conc;   /* theta_d ~ Dir(theta_conc * 1_T) */
+    int32_t K;           /* model topics: initial topics are uniform in [0,K) */
+    int32_t dense_kind;  /* 0: words with count >= K are dense (EZLDA's rule);
+                            1: top dense_param fraction of words; 2: top dense_param words */
+    double dense_param;
+    int32_t num_chunks;  /* contiguous doc ranges with balanced token counts */
+    uint64_t corpus_seed; /* std::mt19937_64 seed of the generative draws */
+    uint64_t topic_seed;  /* Philox seed of the initial topics */
+} lda_gen_config;
+
+typedef struct {
+    int64_t num_tokens; /* N */
+    int64_t vocab;      /* V (words are frequency ranks 0..V-1) */
+    int64_t num_docs;   /* D */
+    int32_t num_chunks; /* C */
+    int32_t num_dense;  /* words [0, num_dense) use the dense word-topic path */
+    int32_t max_doc_len;
+    int32_t K_hint;     /* K the topics were drawn for (0 if unknown) */
+} lda_corpus_info;
+
+/* Array fields readable with lda_corpus_get (element type, count). */
+enum {
+    LDA_F_TOK_WORD = 0,   /* int32 [N]   word of word-sorted token i */
+    LDA_F_TOK_DOC = 1,    /* int32 [N]   global doc of token i */
+    LDA_F_TOPICS = 2,     /* uint16 [N]  initial topic of token i */
+    LDA_F_DOC_OFF = 3,    /* int64 [D+1] doc-order token offsets */
+    LDA_F_DTOK_POS = 4,   /* int64 [N]   word-sorted index of doc-order token j */
+    LDA_F_DTOK_WORD = 5,  /* int32 [N]   word of doc-order token j */
+    LDA_F_CHUNK_TOK = 6,  /* int64 [C+1] first token of each chunk */
+    LDA_F_CHUNK_DOC = 7,  /* int64 [C+1] first doc of each chunk */
+    LDA_F_WORD_COUNT = 8, /* int64 [V]   corpus count of each word */
+    LDA_F_SEG_OFF = 9,    /* int64 [C*V] first token of word w in chunk c (global index) */
+    LDA_F_SEG_CNT = 10    /* int64 [C*V] tokens of word w in chunk c */
+};
+
+int lda_corpus_generate(const lda_gen_config* cfg, lda_corpus** out);
+/* Reads an EZLDA chunk directory (lengthVec.txt, docLength.txt, TLLength.txt,
+ * TLSplit.txt, chunk<c>/{TL,word2DocMap,wordCountOffset,docCountOffset}.txt),
+ * replacing Document::loadDocument / DocChunk::loadChunk (EZLDA/Doc.cu:45-108,
+ * EZLDA/DataChunk.cu:50-100) and WTAll::loadWTCountOffset (EZLDA/WT.cu:155-186). */
+int lda_corpus_load_ezlda(const char* dir, lda_corpus** out);
+/* Writes the EZLDA chunk format (the files preprocess/streamTestBalance.cpp:356-547
+ * writes); K sets the DT/WT capacities the format records. */
+int lda_corpus_write_ezlda(const lda_corpus* c, const char* dir, int32_t K);
+/* Builds the word-sorted chunk layout from doc-ordered tokens: words[j] is the
+ * raw word id (0..V-1) of doc-order token j, doc d owns [doc_off[d], doc_off[d+1]).
+ * Words are renumbered by descending frequency (stable); topics may be NULL
+ * (then drawn from Philox(topic_seed)) and are given in doc order. */
+int lda_corpus_from_docs(int64_t num_docs, const int64_t* doc_off, const int32_t* words,
+                         int64_t vocab, const uint16_t* topics_doc_order, int32_t K,
+                         int32_t num_chunks, int32_t dense_kind, double dense_param,
+                         uint64_t topic_seed, lda_corpus** out);
+int lda_corpus_info_get(const lda_corpus* c, lda_corpus_info* out);
+int lda_corpus_get(const lda_corpus* c, int32_t field, void* out, int64_t count);
+/* Replaces the corpus' initial topics (word-sorted order, 0-based, < K). */
+int lda_corpus_set_topics(lda_corpus* c, const uint16_t* topics, int64_t count);
+void lda_corpus_free(lda_corpus* c);
+
+/* ----------------------------------------------------------------- trainer */
+
+typedef struct {
+    int32_t K;
+    float alpha;            /* EZLDA: 50/K (EZLDA/Argument.cuh:9) */
+    float beta;             /* EZLDA: 0.01 (EZLDA/Argument.cuh:8) */
+    uint64_t seed;          /* Philox seed of the sweep randoms */
+    int32_t device;         /* CUDA device ordinal */
+    int64_t device_budget;  /* bytes the trainer may allocate (0: no limit) */
+} lda_train_config;
+
+/* Per-sweep counters of the last lda_trainer_iterate / lda_sample_chunk calls. */
+typedef struct {
+    int64_t tokens;        /* tokens sampled */
+    int64_t early_accept;  /* settled by the max-topic bound */
+    int64_t full;          /* S evaluated over the doc row */
+    int64_t sum_nnz_full;  /* doc-row entries read by evaluated tokens */
+    int64_t branch_max, branch_s, branch_q;
+    int64_t sum_word_nnz;  /* sparse word-row entries read building word columns */
+    int64_t word_tiles_dense, word_tiles_sparse;
+} lda_sweep_counters;
+
+/* Accumulated device time (CUDA events on the trainer's stream) per stage. */
+typedef struct {
+    double ms_wt;      /* word-topic + topic-total rebuild */
+    double ms_stats;   /* per-word max topics / Q */
+    double ms_dt;      /* doc-topic rebuild + per-token metadata */
+    double ms_sample;  /* sampler */
+    double ms_ll;      /* log-likelihood reduction */
+    double ms_copy;    /* host<->device copies of lda_iterate_host */
+    int64_t launches_wt, launches_stats, launches_dt, launches_sample, launches_ll;
+} lda_stage_timing;
+
+/* Allocates the device copy of the corpus (Document/DTChunk/WTAll/WTD
+ * GPUMemAllocate, EZLDA/Doc.cu:179-246, DT.cu:53-70, WT.cu:76-97,
+ * WTDense.cu:27-43) and uploads it.  Fails with LDA_ERR_DEVICE_MEM when the
+ * allocation would exceed cfg->device_budget or cudaMalloc fails. */
+int lda_trainer_create(const lda_corpus* c, const lda_train_config* cfg, lda_trainer** out);
+int lda_trainer_destroy(lda_trainer* t);
+/* Makes the trainer launch on an external cudaStream_t (NULL: its own stream). */
+int lda_trainer_set_stream(lda_trainer* t, void* cuda_stream);
+int lda_trainer_get_stream(lda_trainer* t, void** cuda_stream);
+/* Bytes of device memory held by the trainer. */
+int lda_trainer_device_bytes(const lda_trainer* t, int64_t* bytes);
+
+/* n full sweeps of the driver loop EZLDA/mainKernel.cu:158-380 on resident
+ * data; ll_mode=1 also evaluates the FP64 log-likelihood of every sweep.
+ * Blocks until the sweeps finish. */
+int lda_trainer_iterate(lda_trainer* t, int32_t n_iters, int32_t ll_mode);
+/* End-to-end sweep through host buffers: uploads topics_in (word-sorted, N),
+ * runs one sweep, downloads the new topics to topics_out and the LL sum to
+ * *ll_sum (when ll_mode), as EZLDA's per-chunk Document::CPU2GPU /
+ * Document::GPU2CPU (EZLDA/Doc.cu:266-308) do around every sweep. */
+int lda_iterate_host(lda_trainer* t, const uint16_t* topics_in, uint16_t* topics_out,
+                     int32_t ll_mode, double* ll_sum);
+/* FP64 sum and token count of the last log-likelihood evaluation; EZLDA's
+ * PerplexityKernel / LDATrainPerplexityReduce (EZLDA/SamplingKernel.cu:172-180,
+ * profilePerp/utility.cu:2883-2925).  Mean per-token LL = ll_sum / n_tokens. */
+int lda_trainer_loglik(lda_trainer* t, double* ll_sum, int64_t* n_tokens);
+int lda_trainer_get_topics(lda_trainer* t, uint16_t* out, int64_t count);
+int lda_trainer_set_topics(lda_trainer* t, const uint16_t* in, int64_t count);
+int lda_trainer_get_iteration(const lda_trainer* t, uint32_t* iter);
+int lda_trainer_set_iteration(lda_trainer* t, uint32_t iter);
+int lda_trainer_counters(lda_trainer* t, lda_sweep_counters* out);
+int lda_trainer_set_timing(lda_trainer* t, int32_t enabled);
+int lda_trainer_timing(lda_trainer* t, lda_stage_timing* out);
+int lda_trainer_reset_stats(lda_trainer* t);
+
+/* Checkpoint = (topics, iteration, seed): every count is a function of the
+ * topics and every random of (seed, iteration, token), so resume is exact. */
+int lda_trainer_checkpoint(lda_trainer* t, const char* path);
+int lda_trainer_restore(lda_trainer* t, const char* path);
+
+/* -------------------------------------------- stage entry points (L2 layer) */
+/* Each runs one stage of a sweep on the trainer's stream (asynchronously). */
+
+/* Rebuilds the dense and sparse word-topic counts and the topic totals n_k
+ * from the current topics.  Replaces UpdateWTDenKernel + UpdateWTDenRowSumKernel
+ * (EZLDA/WTDenUpdateKernel.cuh:25-26), UpdateWTKernel (EZLDA/WTUpdateKernel.cuh:23)
+ * and WTAdditionKernel (EZLDA/WTAddKernel.cuh:24). */
+int lda_update_wt(lda_trainer* t);
+/* Per-word max / 2nd / 3rd topic of phi and the Q bucket.  Replaces
+ * MaxTopicKernel (EZLDA/SamplingKernel.cuh:12). */
+int lda_max_topic(lda_trainer* t);
+/* Doc-topic rows of one chunk plus each token's counts of its word's max and
+ * 2nd topic.  Replaces UpdateDTKernel (EZLDA/DTUpdateKernel.cuh:13). */
+int lda_update_dt(lda_trainer* t, int32_t chunk);
+/* Samples every token of one chunk (dense and sparse words, early accept and
+ * full evaluation in one kernel).  Replaces UpdateProbKernelD, SampleKernelD
+ * and SampleKernel (EZLDA/SamplingKernel.cuh:10-14). */
+int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode);
+/* Reduces the per-tile LL partials of the sampled chunks to *ll_sum (blocks).
+ * Replaces PerplexityKernel (EZLDA/SamplingKernel.cuh:15). */
+int lda_perplexity(lda_trainer* t, double* ll_sum);
+/* Advances the sweep counter (the iteration key of the randoms). */
+int lda_end_sweep(lda_trainer* t);
+int lda_trainer_sync(lda_trainer* t);
+
+/* Device-state readback (blocking copies into caller buffers). */
+int lda_get_topic_totals(lda_trainer* t, int32_t* n_k /*K*/);
+int lda_get_dense_wt(lda_trainer* t, int32_t* out /*num_dense*K*/);
+/* Sparse word rows (words num_dense..V-1) compacted: off has V-num_dense+1
+ * entries, ent holds (k<<16 | count) ascending k.  Returns entries or <0. */
+int64_t lda_get_sparse_wt(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap);
+int lda_get_word_stats(lda_trainer* t, uint32_t* top2, uint32_t* k3, float* phi4, float* ql);
+/* Doc rows of every doc (valid for chunks whose lda_update_dt ran). */
+int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap);
+int lda_get_token_meta(lda_trainer* t, uint32_t* meta /*N*/);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

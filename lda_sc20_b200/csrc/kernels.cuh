@@ -1,0 +1,534 @@
+// kernels.cuh -- sm_100a kernels of the collapsed-Gibbs sweep.
+//
+// Every float operation below is an explicit round-to-nearest intrinsic, so the compiler
+// cannot contract or reorder it.  The sampling arithmetic (summation orders, bin order,
+// tie rules) is the specification the CPU oracle restates; the CUDA path and the oracle
+// therefore draw identical topics for identical (seed, iteration, token).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lda {
+namespace dev {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float u2f(uint32_t x) { return __uint2float_rn(x); }
+
+// Inclusive Kogge-Stone scan over the warp: round `off` adds lane l-off into lane l.
+__device__ __forceinline__ float warp_ks_scan(float v, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const float t = __shfl_up_sync(FULL, v, off);
+        if (lane >= off) v = fadd(v, t);
+    }
+    return v;
+}
+
+// Philox4x32-10 (Salmon et al., SC'11), first output word.
+__device__ __forceinline__ uint32_t philox_x0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c1 = lo1;
+        c3 = lo0;
+        c0 = n0;
+        c2 = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c0;
+}
+
+// u in [0,1) of token `tok` at sweep `iter` (replaces curand_uniform()/1.00001,
+// EZLDA/utility.cu:1353).
+__device__ __forceinline__ float token_uniform(uint32_t seed_lo, uint32_t seed_hi, uint32_t iter,
+                                               uint32_t tok) {
+    const uint32_t x = philox_x0(tok, 0u, iter, 0x4C444131u, seed_lo, seed_hi);
+    return u2f(x >> 8) * 0x1p-24f;
+}
+
+// ---------------------------------------------------------------- WT rebuild
+// Warp per word tile: the tile's topics are histogrammed in a warp-private shared row
+// (match_any-aggregated shared atomics, so a word whose tokens share a topic costs one
+// atomic per distinct topic per 32 tokens).  Dense tiles add their row into the dense
+// word-topic matrix; a sparse word (one tile over all chunks) is compacted to
+// (k<<16 | count) ascending k.  Topic totals n_k are privatised per CTA and flushed once.
+// Replaces WTDen_Update_Kernel, WT_Update_Kernel, sparseMatrixAdd and
+// WTDen_Sum_Update_Kernel (EZLDA/utility.cu:1067-1102, :10-76, :1132-1204, :1104-1126).
+struct WtArgs {
+    const int4* tiles;  // {word, start, count, dense}
+    int ntiles;
+    unsigned* tile_counter;
+    const uint16_t* z;
+    int K, V, Vd, C;
+    const uint32_t* seg_off;  // [C*V]
+    const uint32_t* seg_cnt;  // [C*V]
+    int* dwt;                 // [Vd*K]
+    const uint32_t* swt_off;  // [V-Vd]
+    uint32_t* swt_nnz;
+    uint32_t* swt_ent;
+    int* n_k;
+    int* err;
+};
+
+__device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uint32_t start, uint32_t cnt,
+                                             uint32_t* hist, int K, int lane, int* err) {
+    for (uint32_t base = 0; base < cnt; base += 32) {
+        const uint32_t i = base + lane;
+        bool valid = i < cnt;
+        uint32_t k = valid ? (uint32_t)__ldg(z + start + i) : 0xffffffffu;
+        if (valid && k >= (uint32_t)K) {
+            atomicOr(err, 1);
+            valid = false;
+            k = 0xfffffffeu;
+        }
+        const unsigned m = __match_any_sync(FULL, k);
+        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
+    extern __shared__ uint32_t smu[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* nk = smu;
+    uint32_t* hist = smu + (size_t)a.K * (1 + wid);
+    for (int i = threadIdx.x; i < a.K * (warps + 1); i += blockDim.x) smu[i] = 0u;
+    __syncthreads();
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= a.ntiles) break;
+        const int4 t = a.tiles[tile];
+        const int w = t.x;
+        if (t.w & 1) {
+            hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, a.K, lane, a.err);
+        } else {
+            for (int c = 0; c < a.C; ++c) {
+                const size_t idx = (size_t)c * a.V + w;
+                hist_segment(a.z, a.seg_off[idx], a.seg_cnt[idx], hist, a.K, lane, a.err);
+            }
+        }
+        __syncwarp();
+        if (t.w & 1) {
+            int* row = a.dwt + (size_t)w * a.K;
+            for (int k = lane; k < a.K; k += 32) {
+                const uint32_t h = hist[k];
+                if (h) {
+                    atomicAdd(row + k, (int)h);
+                    atomicAdd(&nk[k], h);
+                    hist[k] = 0u;
+                }
+            }
+        } else {
+            const int s = w - a.Vd;
+            uint32_t* out = a.swt_ent + a.swt_off[s];
+            uint32_t nnz = 0;
+            for (int kb = 0; kb < a.K; kb += 32) {
+                const int k = kb + lane;
+                const uint32_t h = k < a.K ? hist[k] : 0u;
+                const unsigned b = __ballot_sync(FULL, h != 0u);
+                if (h) {
+                    out[nnz + __popc(b & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+                    atomicAdd(&nk[k], h);
+                    hist[k] = 0u;
+                }
+                nnz += (uint32_t)__popc(b);
+            }
+            if (lane == 0) a.swt_nnz[s] = nnz;
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+        const uint32_t v = nk[k];
+        if (v) atomicAdd(a.n_k + k, (int)v);
+    }
+}
+
+// ------------------------------------------------------------ word columns
+// phi_k = ((float)n_wk + beta) * r_k into a warp-private shared row (EZLDA builds the
+// same column as WTHead, utility.cu:1257-1269 sparse, :1698-1702 dense).
+__device__ __forceinline__ void build_column(float* col, const float* r, int w, int Vd, int K, float beta,
+                                             const int* __restrict__ dwt, const uint32_t* __restrict__ swt_off,
+                                             const uint32_t* __restrict__ swt_nnz,
+                                             const uint32_t* __restrict__ swt_ent, int lane, uint32_t* nnz_read) {
+    if (w < Vd) {
+        const int* row = dwt + (size_t)w * K;
+        for (int k = lane; k < K; k += 32) col[k] = fmul(fadd(__int2float_rn(__ldg(row + k)), beta), r[k]);
+    } else {
+        for (int k = lane; k < K; k += 32) col[k] = fmul(beta, r[k]);
+        __syncwarp();
+        const int s = w - Vd;
+        const uint32_t off = __ldg(swt_off + s), nnz = __ldg(swt_nnz + s);
+        for (uint32_t e = lane; e < nnz; e += 32) {
+            const uint32_t en = __ldg(swt_ent + off + e);
+            const uint32_t k = en >> 16;
+            col[k] = fmul(fadd(u2f(en & 0xffffu), beta), r[k]);
+        }
+        if (nnz_read && lane == 0) *nnz_read += nnz;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void warp_argmax(float& v, int& k) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(FULL, v, off);
+        const int ok = __shfl_xor_sync(FULL, k, off);
+        if (ov > v || (ov == v && ok < k)) {
+            v = ov;
+            k = ok;
+        }
+    }
+}
+
+__device__ __forceinline__ void fill_recip(float* r, const int* __restrict__ n_k, int K, float Vbeta) {
+    for (int k = threadIdx.x; k < K; k += blockDim.x) r[k] = __fdiv_rn(1.0f, fadd(__int2float_rn(n_k[k]), Vbeta));
+}
+
+// ---------------------------------------------------------------- word stats
+// Warp per word: max / 2nd / 3rd topic of phi (ties to the lower k), phi at those
+// topics, and the 32 lane partials of Q = alpha * sum_{k != max} phi_k.  Replaces
+// MaxTopicDense_Update_Kernel / MaxTopicSparse_Update_Kernel (EZLDA/utility.cu:305-1062).
+struct StatsArgs {
+    int V, Vd, K;
+    float alpha, beta, Vbeta;
+    const int* n_k;
+    const int* dwt;
+    const uint32_t* swt_off;
+    const uint32_t* swt_nnz;
+    const uint32_t* swt_ent;
+    uint32_t* st_top2;  // (k2 << 16) | maxK
+    uint32_t* st_k3;
+    float4* st_phi;     // {phi_max, phi_2nd, phi_3rd, Q}
+    float* st_ql;       // [V*32]
+};
+
+__global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
+    extern __shared__ float smf[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* r = smf;
+    float* col = smf + (size_t)a.K * (1 + wid);
+    fill_recip(r, a.n_k, a.K, a.Vbeta);
+    __syncthreads();
+    for (int w = blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
+        build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, nullptr);
+        float v1 = -1.0f;
+        int k1 = 0x7fffffff;
+        for (int k = lane; k < a.K; k += 32) if (col[k] > v1) { v1 = col[k]; k1 = k; }
+        warp_argmax(v1, k1);
+        float v2 = -1.0f;
+        int k2 = 0x7fffffff;
+        for (int k = lane; k < a.K; k += 32) if (k != k1 && col[k] > v2) { v2 = col[k]; k2 = k; }
+        warp_argmax(v2, k2);
+        float v3 = -1.0f;
+        int k3 = 0x7fffffff;
+        for (int k = lane; k < a.K; k += 32) if (k != k1 && k != k2 && col[k] > v3) { v3 = col[k]; k3 = k; }
+        warp_argmax(v3, k3);
+        float ql = 0.0f;
+        for (int k = lane; k < a.K; k += 32) if (k != k1) ql = ffma(a.alpha, col[k], ql);
+        const float qp = warp_ks_scan(ql, lane);
+        const float Q = __shfl_sync(FULL, qp, 31);
+        a.st_ql[(size_t)w * 32 + lane] = ql;
+        if (lane == 0) {
+            a.st_top2[w] = ((uint32_t)k2 << 16) | (uint32_t)k1;
+            a.st_k3[w] = (uint32_t)k3;
+            a.st_phi[w] = make_float4(v1, v2, v3, Q);
+        }
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------- DT rebuild
+// Warp per doc of one chunk: the doc's topics are gathered through the doc-order ->
+// word-sorted map into a warp-private shared histogram, each token's counts of its
+// word's max / 2nd topic are scattered to its word-sorted slot, and the histogram is
+// compacted to (k<<16 | count) ascending k.  Replaces DT_Update_Kernel
+// (EZLDA/utility.cu:79-284).
+struct DtArgs {
+    uint32_t d_begin, d_end;
+    int K;
+    const uint32_t* doc_off;    // [D+1] doc-order token offsets
+    const uint32_t* dtok_pos;   // [N]
+    const uint32_t* dtok_word;  // [N]
+    const uint16_t* z;
+    const uint32_t* st_top2;
+    const uint32_t* dt_off;
+    uint32_t* dt_nnz;
+    uint32_t* dt_ent;
+    uint32_t* meta;             // [N] word-sorted: (n_d,2nd << 16) | n_d,max
+    int* err;
+};
+
+__global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
+    extern __shared__ uint32_t smu[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* hist = smu + (size_t)a.K * wid;
+    for (int i = threadIdx.x; i < a.K * warps; i += blockDim.x) smu[i] = 0u;
+    __syncthreads();
+    for (uint32_t d = a.d_begin + blockIdx.x * warps + wid; d < a.d_end; d += gridDim.x * warps) {
+        const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
+        for (uint32_t base = 0; base < n; base += 32) {
+            bool valid = base + lane < n;
+            uint32_t k = valid ? (uint32_t)__ldg(a.z + __ldg(a.dtok_pos + b + base + lane)) : 0xffffffffu;
+            if (valid && k >= (uint32_t)a.K) {
+                atomicOr(a.err, 1);
+                valid = false;
+                k = 0xfffffffeu;
+            }
+            const unsigned m = __match_any_sync(FULL, k);
+            if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+        }
+        __syncwarp();
+        for (uint32_t i = lane; i < n; i += 32) {
+            const uint32_t pos = __ldg(a.dtok_pos + b + i);
+            const uint32_t t2 = __ldg(a.st_top2 + __ldg(a.dtok_word + b + i));
+            const uint32_t k1 = t2 & 0xffffu, k2 = t2 >> 16;
+            const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
+            a.meta[pos] = (c2 << 16) | c1;
+        }
+        __syncwarp();
+        uint32_t* out = a.dt_ent + __ldg(a.dt_off + d);
+        uint32_t nnz = 0;
+        for (int kb = 0; kb < a.K; kb += 32) {
+            const int k = kb + lane;
+            const uint32_t h = k < a.K ? hist[k] : 0u;
+            const unsigned bal = __ballot_sync(FULL, h != 0u);
+            if (h) {
+                out[nnz + __popc(bal & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+                hist[k] = 0u;
+            }
+            nnz += (uint32_t)__popc(bal);
+        }
+        if (lane == 0) a.dt_nnz[d] = nnz;
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------- sampler
+// Warp per (word, token range) tile.  The word's phi column (with phi_max zeroed) sits in
+// warp-private shared memory.  Each 32-token group is first screened thread-per-token by
+// the max-topic bound; tokens that fail it (all tokens in LL mode) are then evaluated one
+// at a time by the whole warp: 4-entry vector loads of the doc row, per-lane partial S,
+// one Kogge-Stone scan, ballot bin search, single-lane refinement.  Replaces
+// UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain (EZLDA/utility.cu:2680-3312,
+// :1625-2103, :1217-1611) in one pass, with no effective-token list and no spin lock.
+struct SampleArgs {
+    const int4* tiles;  // {word, start, count, dense}
+    int ntiles;
+    unsigned* tile_counter;
+    double* tile_ll;
+    int K, Vd, ll_mode;
+    float alpha, beta, Vbeta;
+    double den_add;  // (double)K * (double)alpha
+    uint32_t seed_lo, seed_hi, iter;
+    const int* n_k;
+    const int* dwt;
+    const uint32_t* swt_off;
+    const uint32_t* swt_nnz;
+    const uint32_t* swt_ent;
+    const uint32_t* st_top2;
+    const float4* st_phi;
+    const float* st_ql;
+    const uint32_t* tok_doc;
+    const uint32_t* meta;
+    uint16_t* z;
+    const uint32_t* doc_len;
+    const uint32_t* dt_off;
+    const uint32_t* dt_nnz;
+    const uint32_t* dt_ent;
+    unsigned long long* ctr;  // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles
+};
+
+__global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
+    extern __shared__ float smf[];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* r = smf;
+    float* col = smf + (size_t)a.K * (1 + wid);
+    fill_recip(r, a.n_k, a.K, a.Vbeta);
+    __syncthreads();
+    uint32_t c_tok = 0, c_ea = 0, c_full = 0, c_nnz = 0, c_max = 0, c_s = 0, c_q = 0, c_wnnz = 0;
+    uint32_t c_tdense = 0, c_tsparse = 0;
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= a.ntiles) break;
+        const int4 t = a.tiles[tile];
+        const int w = t.x;
+        const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
+        __syncwarp();
+        build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &c_wnnz);
+        if (lane == 0) {
+            c_tdense += (w < a.Vd);
+            c_tsparse += (w >= a.Vd);
+        }
+        const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
+        const float4 ph = __ldg(a.st_phi + w);
+        const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
+        const float QP = warp_ks_scan(QL, lane);
+        const float Q = __shfl_sync(FULL, QP, 31);
+        if (lane == 0) col[maxK] = 0.0f;
+        __syncwarp();
+        double ll = 0.0;
+        for (uint32_t g = 0; g < cnt; g += 32) {
+            const bool valid = g + lane < cnt;
+            const uint32_t tok = start + g + lane;
+            uint32_t d = 0, nd = 0;
+            float u = 0.0f, pmax = 0.0f;
+            bool ea = false;
+            if (valid) {
+                d = __ldg(a.tok_doc + tok);
+                const uint32_t m = __ldg(a.meta + tok);
+                nd = __ldg(a.doc_len + d);
+                const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
+                u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
+                pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
+                const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
+                const float bound = fadd(fadd(pmax, shat), Q);
+                ea = fmul(u, bound) < pmax;
+                c_tok++;
+                c_ea += ea;
+            }
+            int znew = maxK;
+            unsigned need = __ballot_sync(FULL, valid && (!ea || a.ll_mode));
+            while (need) {
+                const int j = __ffs(need) - 1;
+                need &= need - 1u;
+                const uint32_t dj = __shfl_sync(FULL, d, j);
+                const uint32_t ndj = __shfl_sync(FULL, nd, j);
+                const float pmj = __shfl_sync(FULL, pmax, j);
+                const float uj = __shfl_sync(FULL, u, j);
+                const int eaj = __shfl_sync(FULL, (int)ea, j);
+                const uint32_t nnz = __ldg(a.dt_nnz + dj);
+                const uint32_t* row = a.dt_ent + __ldg(a.dt_off + dj);
+                float SL = 0.0f;
+                for (uint32_t q = 4u * lane; q < nnz; q += 128u) {
+                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
+                    SL = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], SL);
+                    if (q + 1 < nnz) SL = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], SL);
+                    if (q + 2 < nnz) SL = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], SL);
+                    if (q + 3 < nnz) SL = ffma(u2f(v.w & 0xffffu), col[v.w >> 16], SL);
+                }
+                const float SP = warp_ks_scan(SL, lane);
+                const float S = __shfl_sync(FULL, SP, 31);
+                const float pS = fadd(pmj, S);
+                const float total = fadd(pS, Q);
+                if (lane == 0) {
+                    c_full++;
+                    c_nnz += nnz;
+                }
+                if (a.ll_mode && lane == j) ll += log((double)total / ((double)ndj + a.den_add));
+                if (!eaj) {
+                    const float target = fmul(uj, total);
+                    int zj;
+                    if (target < pmj) {
+                        zj = maxK;
+                        c_max += (lane == 0);
+                    } else if (target < pS) {
+                        const float tt = fsub(target, pmj);
+                        const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
+                        const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
+                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                        const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
+                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                        int found = -1, last = -1;
+                        if (lane == ls) {
+                            float acc = 0.0f;
+                            for (uint32_t q = 4u * ls; q < nnz && found < 0; q += 128u) {
+                                const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
+                                const uint32_t e4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+                                for (int i = 0; i < 4; ++i) {
+                                    if (q + i < nnz && found < 0) {
+                                        const uint32_t k = e4[i] >> 16;
+                                        const float cz = col[k];
+                                        acc = ffma(u2f(e4[i] & 0xffffu), cz, acc);
+                                        if (cz > 0.0f) {
+                                            last = (int)k;
+                                            if (t2 < acc) found = (int)k;
+                                        }
+                                    }
+                                }
+                            }
+                        }
+                        zj = __shfl_sync(FULL, found >= 0 ? found : last, ls & 31);
+                        if (ls < 0 || zj < 0) zj = maxK;
+                        c_s += (lane == 0);
+                    } else {
+                        const float tt = fsub(target, pS);
+                        const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
+                        const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
+                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                        const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
+                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                        int found = -1, last = -1;
+                        if (lane == ls) {
+                            float acc = 0.0f;
+                            for (int k = ls; k < a.K; k += 32) {
+                                const float cz = col[k];
+                                acc = ffma(a.alpha, cz, acc);
+                                if (cz > 0.0f) {
+                                    last = k;
+                                    if (t2 < acc) {
+                                        found = k;
+                                        break;
+                                    }
+                                }
+                            }
+                        }
+                        zj = __shfl_sync(FULL, found >= 0 ? found : last, ls & 31);
+                        if (ls < 0 || zj < 0) zj = maxK;
+                        c_q += (lane == 0);
+                    }
+                    if (lane == j) znew = zj;
+                } else {
+                    c_max += (lane == 0);
+                }
+            }
+            if (valid) {
+                if (ea && !a.ll_mode) c_max++;
+                a.z[tok] = (uint16_t)znew;
+            }
+        }
+        if (a.ll_mode) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);
+            if (lane == 0) a.tile_ll[tile] = ll;
+        }
+    }
+    const uint32_t vals[10] = {c_tok, c_ea, c_full, c_nnz, c_max, c_s, c_q, c_wnnz, c_tdense, c_tsparse};
+#pragma unroll
+    for (int i = 0; i < 10; ++i) {
+        const uint32_t s = __reduce_add_sync(FULL, vals[i]);
+        if (lane == 0 && s) atomicAdd(a.ctr + i, (unsigned long long)s);
+    }
+}
+
+// Fixed-order FP64 reduction of the per-tile LL partials (one CTA of 1024 threads).
+// Replaces LDATrainPerplexityReduce (EZLDA/utility.cu:2106-2151).
+__global__ void __launch_bounds__(1024) k_ll_reduce(const double* __restrict__ in, int n, double* out) {
+    __shared__ double s[1024];
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += in[i];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
+        if ((int)threadIdx.x < h) s[threadIdx.x] += s[threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = s[0];
+}
+
+}  // namespace dev
+}  // namespace lda

@@ -1,0 +1,721 @@
+// trainer.cu -- device state, stage launches and the C ABI of the sweep.
+//
+// Driver semantics follow EZLDA/mainKernel.cu:158-380: every count a sweep reads is a
+// snapshot of the sweep's starting topics (word-topic counts and n_k rebuilt first, the
+// doc-topic rows of each chunk rebuilt from that chunk's topics before it is sampled), and
+// new topics are written in place.  Unlike EZLDA, which re-uploads every chunk each
+// sweep, the corpus stays resident in HBM (72M tokens use ~1.5 GB of a B200's 180 GB);
+// chunks remain the unit of the doc-topic rebuild so that one chunk's doc rows stay
+// L2-resident between the rebuild and the sampler.
+#include <algorithm>
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "common.h"
+#include "kernels.cuh"
+
+using namespace lda;
+
+namespace {
+
+constexpr int kSampleTile = 4096;  // tokens per sampler tile (a word's column is rebuilt per tile)
+constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
+constexpr int kCounters = 16;
+
+struct EventPair {
+    cudaEvent_t a = nullptr, b = nullptr;
+    int stage = 0;
+};
+
+}  // namespace
+
+struct lda_trainer {
+    int device = 0;
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    int K = 0, Vd = 0, C = 0, warps = 8, num_sms = 0;
+    float alpha = 0, beta = 0, Vbeta = 0;
+    uint64_t seed = 0;
+    uint32_t iter = 0;
+    int64_t N = 0, V = 0, D = 0;
+    std::vector<int64_t> chunk_tok, chunk_doc;
+    std::vector<int> s_tile_base;  // [C+1]
+    int n_wtiles = 0;
+
+    // device arrays
+    uint32_t *tok_doc = nullptr, *meta = nullptr, *dtok_pos = nullptr, *dtok_word = nullptr;
+    uint32_t *doc_off = nullptr, *doc_len = nullptr, *dt_off = nullptr, *dt_nnz = nullptr, *dt_ent = nullptr;
+    uint16_t* z = nullptr;
+    int* dwt = nullptr;
+    uint32_t *swt_off = nullptr, *swt_nnz = nullptr, *swt_ent = nullptr;
+    int* n_k = nullptr;
+    uint32_t *st_top2 = nullptr, *st_k3 = nullptr;
+    float4* st_phi = nullptr;
+    float* st_ql = nullptr;
+    uint32_t *seg_off = nullptr, *seg_cnt = nullptr;
+    int4 *s_tiles = nullptr, *w_tiles = nullptr;
+    double *tile_ll = nullptr, *ll_dev = nullptr;
+    unsigned* tile_ctr = nullptr;         // [1 + C]
+    unsigned long long* ctr = nullptr;    // [kCounters]
+    int* err = nullptr;
+    double* ll_host = nullptr;            // pinned
+
+    int64_t dt_cap = 0, swt_cap = 0;
+    size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0;
+    int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0;
+
+    std::vector<void*> allocs;
+    int64_t bytes = 0, budget = 0;
+
+    bool timing = false;
+    std::vector<EventPair> pending, pool;
+    lda_stage_timing tm{};
+
+    double last_ll = 0.0;
+    int64_t last_ll_tokens = 0;
+    bool ll_valid = false;
+    std::vector<bool> chunk_sampled_ll;
+
+    ~lda_trainer() {
+        if (device >= 0) cudaSetDevice(device);
+        if (stream) cudaStreamSynchronize(stream);
+        for (void* p : allocs) cudaFree(p);
+        if (ll_host) cudaFreeHost(ll_host);
+        for (auto& e : pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+        for (auto& e : pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    template <class T>
+    int alloc(T** p, int64_t count) {
+        const int64_t b = std::max<int64_t>(count, 1) * (int64_t)sizeof(T);
+        if (budget > 0 && bytes + b > budget)
+            return fail(LDA_ERR_DEVICE_MEM, "device budget of %lld bytes exceeded (need %lld more, hold %lld)",
+                        (long long)budget, (long long)b, (long long)bytes);
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, (size_t)b);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LDA_ERR_DEVICE_MEM, "cudaMalloc of %lld bytes failed: %s", (long long)b, cudaGetErrorString(e));
+        }
+        allocs.push_back(q);
+        bytes += b;
+        *p = (T*)q;
+        return LDA_OK;
+    }
+
+    EventPair* begin_stage(int stage) {
+        if (!timing) return nullptr;
+        EventPair e;
+        if (!pool.empty()) { e = pool.back(); pool.pop_back(); }
+        else { cudaEventCreate(&e.a); cudaEventCreate(&e.b); }
+        e.stage = stage;
+        cudaEventRecord(e.a, stream);
+        pending.push_back(e);
+        return &pending.back();
+    }
+    void end_stage() {
+        if (!timing || pending.empty()) return;
+        cudaEventRecord(pending.back().b, stream);
+    }
+    void collect_timing() {
+        for (auto& e : pending) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e.a, e.b);
+            switch (e.stage) {
+                case 0: tm.ms_wt += ms; tm.launches_wt++; break;
+                case 1: tm.ms_stats += ms; tm.launches_stats++; break;
+                case 2: tm.ms_dt += ms; tm.launches_dt++; break;
+                case 3: tm.ms_sample += ms; tm.launches_sample++; break;
+                case 4: tm.ms_ll += ms; tm.launches_ll++; break;
+                default: tm.ms_copy += ms; break;
+            }
+            pool.push_back(e);
+        }
+        pending.clear();
+    }
+};
+
+#define CUDA_TRY(expr)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (expr);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            cudaGetLastError();                                                                \
+            return fail(LDA_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));         \
+        }                                                                                      \
+    } while (0)
+
+extern "C" const char* lda_version(void) { return "lda_b200 1.0 (sm_100a)"; }
+
+static int occupancy_grid(const void* fn, int threads, size_t smem, int num_sms, int* grid) {
+    int per_sm = 0;
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, smem));
+    if (per_sm < 1) return fail(LDA_ERR_CUDA, "kernel cannot be resident with %zu bytes of shared memory", smem);
+    *grid = per_sm * num_sms;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* cfg, lda_trainer** out) {
+    if (!c || !cfg || !out) return fail(LDA_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->K < 4 || cfg->K > 65535) return fail(LDA_ERR_ARG, "K=%d outside [4, 65535]", cfg->K);
+    if (!(cfg->alpha > 0.f) || !(cfg->beta > 0.f)) return fail(LDA_ERR_ARG, "alpha and beta must be > 0");
+    if (cfg->device_budget < 0) return fail(LDA_ERR_ARG, "negative device budget");
+    for (int64_t i = 0; i < c->N; ++i)
+        if (c->z[i] >= cfg->K) return fail(LDA_ERR_ARG, "initial topic %d of token %lld >= K=%d", c->z[i], (long long)i, cfg->K);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(LDA_ERR_CUDA, "no CUDA device available");
+    }
+    if (cfg->device < 0 || cfg->device >= ndev) return fail(LDA_ERR_ARG, "device %d of %d", cfg->device, ndev);
+    std::unique_ptr<lda_trainer> t(new lda_trainer());
+    lda_trainer& T = *t;
+    T.device = cfg->device;
+    CUDA_TRY(cudaSetDevice(T.device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&T.own_stream, cudaStreamNonBlocking));
+    T.stream = T.own_stream;
+    CUDA_TRY(cudaDeviceGetAttribute(&T.num_sms, cudaDevAttrMultiProcessorCount, T.device));
+    int max_smem = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, T.device));
+    T.K = cfg->K; T.alpha = cfg->alpha; T.beta = cfg->beta; T.seed = cfg->seed;
+    T.N = c->N; T.V = c->V; T.D = c->D; T.C = c->C; T.Vd = c->V_dense;
+    T.Vbeta = (float)T.V * T.beta;
+    T.budget = cfg->device_budget;
+    T.chunk_tok = c->chunk_tok;
+    T.chunk_doc = c->chunk_doc;
+    // warps per CTA: (warps + 1) K-wide shared rows must fit
+    const int64_t row = (int64_t)T.K * 4;
+    T.warps = (int)std::min<int64_t>(8, (int64_t)max_smem / row - 1);
+    if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
+    T.smem_wt = T.smem_stats = T.smem_sample = (size_t)(T.warps + 1) * row;
+    T.smem_dt = (size_t)T.warps * row;
+
+    // ---- host-side derived layout
+    const int64_t N = T.N, V = T.V, D = T.D, Vs = V - T.Vd;
+    std::vector<uint32_t> h32(std::max<int64_t>({N, D + 1, (int64_t)T.C * V, 1}));
+    // doc rows: capacity roundup4(min(len, K)) keeps every row 16-byte aligned
+    std::vector<uint32_t> hdt_off(D), hdoc_len(D);
+    int64_t run = 0;
+    for (int64_t d = 0; d < D; ++d) {
+        const int64_t len = c->doc_off[d + 1] - c->doc_off[d];
+        hdoc_len[d] = (uint32_t)len;
+        hdt_off[d] = (uint32_t)run;
+        run += (std::min<int64_t>(len, T.K) + 3) & ~int64_t(3);
+    }
+    T.dt_cap = run;
+    if (run >= (int64_t)UINT32_MAX) return fail(LDA_ERR_ARG, "doc-topic storage exceeds 2^32 entries");
+    std::vector<uint32_t> hswt_off(std::max<int64_t>(Vs, 1));
+    run = 0;
+    for (int64_t s = 0; s < Vs; ++s) {
+        hswt_off[s] = (uint32_t)run;
+        run += std::min<int64_t>(c->word_count[T.Vd + s], T.K);
+    }
+    T.swt_cap = run;
+    // sampler tiles per chunk, largest first
+    std::vector<int4> st;
+    T.s_tile_base.assign(T.C + 1, 0);
+    for (int ch = 0; ch < T.C; ++ch) {
+        std::vector<int4> ct;
+        for (int64_t w = 0; w < V; ++w) {
+            const int64_t n = c->seg_cnt[(size_t)ch * V + w], o = c->seg_off[(size_t)ch * V + w];
+            for (int64_t p = 0; p < n; p += kSampleTile)
+                ct.push_back(make_int4((int)w, (int)(o + p), (int)std::min<int64_t>(kSampleTile, n - p), w < T.Vd));
+        }
+        std::stable_sort(ct.begin(), ct.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
+        st.insert(st.end(), ct.begin(), ct.end());
+        T.s_tile_base[ch + 1] = (int)st.size();
+    }
+    // word-topic tiles: dense segments of every chunk, and one tile per sparse word
+    std::vector<int4> wt;
+    for (int64_t w = 0; w < V; ++w) {
+        if (w < T.Vd) {
+            for (int ch = 0; ch < T.C; ++ch) {
+                const int64_t n = c->seg_cnt[(size_t)ch * V + w], o = c->seg_off[(size_t)ch * V + w];
+                for (int64_t p = 0; p < n; p += kWtTile)
+                    wt.push_back(make_int4((int)w, (int)(o + p), (int)std::min<int64_t>(kWtTile, n - p), 1));
+            }
+        } else if (c->word_count[w] > 0) {
+            wt.push_back(make_int4((int)w, 0, (int)c->word_count[w], 0));
+        }
+    }
+    std::stable_sort(wt.begin(), wt.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
+    T.n_wtiles = (int)wt.size();
+
+    // ---- device allocation (Document/DTChunk/WTAll/WTD::GPUMemAllocate)
+    int rc;
+#define ALLOC(p, n) if ((rc = T.alloc(&(p), (n))) != LDA_OK) return rc
+    ALLOC(T.tok_doc, N); ALLOC(T.meta, N); ALLOC(T.dtok_pos, N); ALLOC(T.dtok_word, N); ALLOC(T.z, N);
+    ALLOC(T.doc_off, D + 1); ALLOC(T.doc_len, D); ALLOC(T.dt_off, D); ALLOC(T.dt_nnz, D); ALLOC(T.dt_ent, T.dt_cap);
+    ALLOC(T.dwt, (int64_t)T.Vd * T.K); ALLOC(T.swt_off, std::max<int64_t>(Vs, 1)); ALLOC(T.swt_nnz, std::max<int64_t>(Vs, 1));
+    ALLOC(T.swt_ent, T.swt_cap);
+    ALLOC(T.n_k, T.K); ALLOC(T.st_top2, V); ALLOC(T.st_k3, V); ALLOC(T.st_phi, V); ALLOC(T.st_ql, V * 32);
+    ALLOC(T.seg_off, (int64_t)T.C * V); ALLOC(T.seg_cnt, (int64_t)T.C * V);
+    ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
+    ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
+    ALLOC(T.tile_ctr, 1 + T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
+#undef ALLOC
+    CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
+
+    // ---- upload (synchronous: creation is not on the hot path)
+    auto up32 = [&](uint32_t* dst, int64_t n, auto getter) -> int {
+        for (int64_t i = 0; i < n; ++i) h32[i] = (uint32_t)getter(i);
+        CUDA_TRY(cudaMemcpy(dst, h32.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice));
+        return LDA_OK;
+    };
+    if ((rc = up32(T.tok_doc, N, [&](int64_t i) { return c->tok_doc[i]; }))) return rc;
+    if ((rc = up32(T.dtok_pos, N, [&](int64_t i) { return c->dtok_pos[i]; }))) return rc;
+    if ((rc = up32(T.dtok_word, N, [&](int64_t i) { return c->dtok_word[i]; }))) return rc;
+    if ((rc = up32(T.doc_off, D + 1, [&](int64_t i) { return c->doc_off[i]; }))) return rc;
+    if ((rc = up32(T.seg_off, (int64_t)T.C * V, [&](int64_t i) { return c->seg_off[i]; }))) return rc;
+    if ((rc = up32(T.seg_cnt, (int64_t)T.C * V, [&](int64_t i) { return c->seg_cnt[i]; }))) return rc;
+    CUDA_TRY(cudaMemcpy(T.z, c->z.data(), sizeof(uint16_t) * (size_t)N, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(T.doc_len, hdoc_len.data(), sizeof(uint32_t) * (size_t)D, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(T.dt_off, hdt_off.data(), sizeof(uint32_t) * (size_t)D, cudaMemcpyHostToDevice));
+    if (Vs > 0) CUDA_TRY(cudaMemcpy(T.swt_off, hswt_off.data(), sizeof(uint32_t) * (size_t)Vs, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemset(T.swt_nnz, 0, sizeof(uint32_t) * (size_t)std::max<int64_t>(Vs, 1)));
+    CUDA_TRY(cudaMemset(T.dt_nnz, 0, sizeof(uint32_t) * (size_t)D));
+    CUDA_TRY(cudaMemset(T.meta, 0, sizeof(uint32_t) * (size_t)N));
+    // stats start valid (topic 0) so a stage called out of order reads in-range topics
+    CUDA_TRY(cudaMemset(T.st_top2, 0, sizeof(uint32_t) * (size_t)V));
+    CUDA_TRY(cudaMemset(T.st_k3, 0, sizeof(uint32_t) * (size_t)V));
+    CUDA_TRY(cudaMemset(T.st_phi, 0, sizeof(float4) * (size_t)V));
+    CUDA_TRY(cudaMemset(T.st_ql, 0, sizeof(float) * 32 * (size_t)V));
+    CUDA_TRY(cudaMemset(T.n_k, 0, sizeof(int) * (size_t)T.K));
+    CUDA_TRY(cudaMemset(T.err, 0, sizeof(int)));
+    CUDA_TRY(cudaMemset(T.ctr, 0, sizeof(unsigned long long) * kCounters));
+    CUDA_TRY(cudaMemset(T.tile_ll, 0, sizeof(double) * std::max<size_t>(st.size(), 1)));
+    if (!st.empty()) CUDA_TRY(cudaMemcpy(T.s_tiles, st.data(), sizeof(int4) * st.size(), cudaMemcpyHostToDevice));
+    if (!wt.empty()) CUDA_TRY(cudaMemcpy(T.w_tiles, wt.data(), sizeof(int4) * wt.size(), cudaMemcpyHostToDevice));
+
+    // ---- launch shapes: persistent grids sized by occupancy
+    const int threads = 32 * T.warps;
+    for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
+                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair((const void*)dev::k_sample, T.smem_sample)})
+        CUDA_TRY(cudaFuncSetAttribute(kv.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kv.second));
+    if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
+    if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
+    if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
+    if ((rc = occupancy_grid((const void*)dev::k_sample, threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+    T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
+    CUDA_TRY(cudaDeviceSynchronize());
+    T.chunk_sampled_ll.assign(T.C, false);
+    *out = t.release();
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_destroy(lda_trainer* t) {
+    delete t;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_set_stream(lda_trainer* t, void* s) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    t->stream = s ? (cudaStream_t)s : t->own_stream;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_get_stream(lda_trainer* t, void** s) {
+    if (!t || !s) return fail(LDA_ERR_ARG, "null argument");
+    *s = (void*)t->stream;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_device_bytes(const lda_trainer* t, int64_t* b) {
+    if (!t || !b) return fail(LDA_ERR_ARG, "null argument");
+    *b = t->bytes;
+    return LDA_OK;
+}
+
+// ------------------------------------------------------------------- stages
+
+extern "C" int lda_update_wt(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(0);
+    CUDA_TRY(cudaMemsetAsync(t->n_k, 0, sizeof(int) * (size_t)t->K, t->stream));
+    if (t->Vd > 0) CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
+    CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
+    dev::WtArgs a;
+    a.tiles = t->w_tiles; a.ntiles = t->n_wtiles; a.tile_counter = t->tile_ctr;
+    a.z = t->z; a.K = t->K; a.V = (int)t->V; a.Vd = t->Vd; a.C = t->C;
+    a.seg_off = t->seg_off; a.seg_cnt = t->seg_cnt;
+    a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
+    a.n_k = t->n_k; a.err = t->err;
+    const int grid = std::max(1, std::min(t->grid_wt, (t->n_wtiles + t->warps - 1) / t->warps));
+    dev::k_wt_build<<<grid, 32 * t->warps, t->smem_wt, t->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    t->end_stage();
+    return LDA_OK;
+}
+
+extern "C" int lda_max_topic(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(1);
+    dev::StatsArgs a;
+    a.V = (int)t->V; a.Vd = t->Vd; a.K = t->K; a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
+    a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
+    a.st_top2 = t->st_top2; a.st_k3 = t->st_k3; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
+    dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    t->end_stage();
+    return LDA_OK;
+}
+
+extern "C" int lda_update_dt(lda_trainer* t, int32_t chunk) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(2);
+    dev::DtArgs a;
+    a.d_begin = (uint32_t)t->chunk_doc[chunk]; a.d_end = (uint32_t)t->chunk_doc[chunk + 1]; a.K = t->K;
+    a.doc_off = t->doc_off; a.dtok_pos = t->dtok_pos; a.dtok_word = t->dtok_word; a.z = t->z;
+    a.st_top2 = t->st_top2; a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = t->dt_ent; a.meta = t->meta;
+    a.err = t->err;
+    const int64_t nd = a.d_end - a.d_begin;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps - 1) / t->warps));
+    dev::k_dt_build<<<grid, 32 * t->warps, t->smem_dt, t->stream>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    t->end_stage();
+    return LDA_OK;
+}
+
+extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(3);
+    const int base = t->s_tile_base[chunk], n = t->s_tile_base[chunk + 1] - base;
+    unsigned* ctr = t->tile_ctr + 1 + chunk;
+    CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned), t->stream));
+    dev::SampleArgs a;
+    a.tiles = t->s_tiles + base; a.ntiles = n; a.tile_counter = ctr; a.tile_ll = t->tile_ll + base;
+    a.K = t->K; a.Vd = t->Vd; a.ll_mode = ll_mode ? 1 : 0;
+    a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
+    a.den_add = (double)t->K * (double)t->alpha;
+    a.seed_lo = (uint32_t)t->seed; a.seed_hi = (uint32_t)(t->seed >> 32); a.iter = t->iter;
+    a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
+    a.st_top2 = t->st_top2; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
+    a.tok_doc = t->tok_doc; a.meta = t->meta; a.z = t->z; a.doc_len = t->doc_len;
+    a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = t->dt_ent; a.ctr = t->ctr;
+    if (n > 0) {
+        const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
+        dev::k_sample<<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    }
+    t->end_stage();
+    t->chunk_sampled_ll[chunk] = ll_mode != 0;
+    return LDA_OK;
+}
+
+static int perplexity_async(lda_trainer* t) {
+    t->begin_stage(4);
+    const int n = t->s_tile_base[t->C];
+    dev::k_ll_reduce<<<1, 1024, 0, t->stream>>>(t->tile_ll, n, t->ll_dev);
+    CUDA_TRY(cudaGetLastError());
+    t->end_stage();
+    CUDA_TRY(cudaMemcpyAsync(t->ll_host, t->ll_dev, sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+    return LDA_OK;
+}
+
+static int finish(lda_trainer* t) {
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    t->collect_timing();
+    int herr = 0;
+    CUDA_TRY(cudaMemcpy(&herr, t->err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (herr) {
+        CUDA_TRY(cudaMemset(t->err, 0, sizeof(int)));
+        return fail(LDA_ERR_DEVICE, "a kernel found a topic >= K=%d in the topic array (the tokens were skipped)", t->K);
+    }
+    return LDA_OK;
+}
+
+extern "C" int lda_perplexity(lda_trainer* t, double* ll_sum) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    for (int ch = 0; ch < t->C; ++ch)
+        if (!t->chunk_sampled_ll[ch]) return fail(LDA_ERR_STATE, "chunk %d was not sampled with ll_mode=1", ch);
+    CUDA_TRY(cudaSetDevice(t->device));
+    int rc = perplexity_async(t);
+    if (rc) return rc;
+    if ((rc = finish(t))) return rc;
+    t->last_ll = *t->ll_host;
+    t->last_ll_tokens = t->N;
+    t->ll_valid = true;
+    if (ll_sum) *ll_sum = t->last_ll;
+    return LDA_OK;
+}
+
+extern "C" int lda_end_sweep(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    t->iter++;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_sync(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    return finish(t);
+}
+
+static int sweep_async(lda_trainer* t, int ll_mode) {
+    int rc;
+    if ((rc = lda_update_wt(t))) return rc;
+    if ((rc = lda_max_topic(t))) return rc;
+    for (int ch = 0; ch < t->C; ++ch) {
+        if ((rc = lda_update_dt(t, ch))) return rc;
+        if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
+    }
+    if (ll_mode && (rc = perplexity_async(t))) return rc;
+    t->iter++;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_iterate(lda_trainer* t, int32_t n, int32_t ll_mode) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (n < 0) return fail(LDA_ERR_ARG, "negative iteration count");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaMemsetAsync(t->ctr, 0, sizeof(unsigned long long) * kCounters, t->stream));
+    for (int i = 0; i < n; ++i) {
+        int rc = sweep_async(t, ll_mode);
+        if (rc) return rc;
+    }
+    int rc = finish(t);
+    if (rc) return rc;
+    if (ll_mode && n > 0) {
+        t->last_ll = *t->ll_host;
+        t->last_ll_tokens = t->N;
+        t->ll_valid = true;
+    }
+    return LDA_OK;
+}
+
+extern "C" int lda_iterate_host(lda_trainer* t, const uint16_t* zin, uint16_t* zout, int32_t ll_mode, double* ll_sum) {
+    if (!t || !zin || !zout) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(5);
+    CUDA_TRY(cudaMemcpyAsync(t->z, zin, sizeof(uint16_t) * (size_t)t->N, cudaMemcpyHostToDevice, t->stream));
+    t->end_stage();
+    int rc = sweep_async(t, ll_mode);
+    if (rc) return rc;
+    t->begin_stage(5);
+    CUDA_TRY(cudaMemcpyAsync(zout, t->z, sizeof(uint16_t) * (size_t)t->N, cudaMemcpyDeviceToHost, t->stream));
+    t->end_stage();
+    if ((rc = finish(t))) return rc;
+    if (ll_mode) {
+        t->last_ll = *t->ll_host;
+        t->last_ll_tokens = t->N;
+        t->ll_valid = true;
+        if (ll_sum) *ll_sum = t->last_ll;
+    }
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_loglik(lda_trainer* t, double* ll, int64_t* n) {
+    if (!t || !ll) return fail(LDA_ERR_ARG, "null argument");
+    if (!t->ll_valid) return fail(LDA_ERR_STATE, "no log-likelihood has been evaluated (run a sweep with ll_mode=1)");
+    *ll = t->last_ll;
+    if (n) *n = t->last_ll_tokens;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_get_topics(lda_trainer* t, uint16_t* out, int64_t count) {
+    if (!t || !out || count != t->N) return fail(LDA_ERR_ARG, "bad output buffer (need %lld topics)", (long long)(t ? t->N : 0));
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    CUDA_TRY(cudaMemcpy(out, t->z, sizeof(uint16_t) * (size_t)count, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_set_topics(lda_trainer* t, const uint16_t* in, int64_t count) {
+    if (!t || !in || count != t->N) return fail(LDA_ERR_ARG, "bad input buffer (need %lld topics)", (long long)(t ? t->N : 0));
+    for (int64_t i = 0; i < count; ++i)
+        if (in[i] >= t->K) return fail(LDA_ERR_ARG, "topic %d of token %lld >= K=%d", in[i], (long long)i, t->K);
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    CUDA_TRY(cudaMemcpy(t->z, in, sizeof(uint16_t) * (size_t)count, cudaMemcpyHostToDevice));
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_get_iteration(const lda_trainer* t, uint32_t* it) {
+    if (!t || !it) return fail(LDA_ERR_ARG, "null argument");
+    *it = t->iter;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_set_iteration(lda_trainer* t, uint32_t it) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    t->iter = it;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_counters(lda_trainer* t, lda_sweep_counters* o) {
+    if (!t || !o) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    unsigned long long h[kCounters];
+    CUDA_TRY(cudaMemcpy(h, t->ctr, sizeof(h), cudaMemcpyDeviceToHost));
+    o->tokens = (int64_t)h[0]; o->early_accept = (int64_t)h[1]; o->full = (int64_t)h[2]; o->sum_nnz_full = (int64_t)h[3];
+    o->branch_max = (int64_t)h[4]; o->branch_s = (int64_t)h[5]; o->branch_q = (int64_t)h[6]; o->sum_word_nnz = (int64_t)h[7];
+    o->word_tiles_dense = (int64_t)h[8]; o->word_tiles_sparse = (int64_t)h[9];
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_reset_stats(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    CUDA_TRY(cudaMemset(t->ctr, 0, sizeof(unsigned long long) * kCounters));
+    t->collect_timing();
+    t->tm = lda_stage_timing{};
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_set_timing(lda_trainer* t, int32_t on) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    t->timing = on != 0;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_timing(lda_trainer* t, lda_stage_timing* o) {
+    if (!t || !o) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    t->collect_timing();
+    *o = t->tm;
+    return LDA_OK;
+}
+
+// ---------------------------------------------------------------- checkpoint
+
+namespace {
+struct CkptHeader {
+    char magic[8];
+    uint32_t version, K;
+    uint64_t N, seed;
+    uint32_t iter, pad;
+};
+}  // namespace
+
+extern "C" int lda_trainer_checkpoint(lda_trainer* t, const char* path) {
+    if (!t || !path) return fail(LDA_ERR_ARG, "null argument");
+    std::vector<uint16_t> z((size_t)t->N);
+    int rc = lda_trainer_get_topics(t, z.data(), t->N);
+    if (rc) return rc;
+    CkptHeader h{};
+    std::memcpy(h.magic, "LDAB200", 8);
+    h.version = 1; h.K = (uint32_t)t->K; h.N = (uint64_t)t->N; h.seed = t->seed; h.iter = t->iter;
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(LDA_ERR_IO, "cannot open %s for writing", path);
+    bool ok = std::fwrite(&h, sizeof(h), 1, f) == 1 && std::fwrite(z.data(), sizeof(uint16_t), z.size(), f) == z.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? LDA_OK : fail(LDA_ERR_IO, "short write to %s", path);
+}
+
+extern "C" int lda_trainer_restore(lda_trainer* t, const char* path) {
+    if (!t || !path) return fail(LDA_ERR_ARG, "null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(LDA_ERR_IO, "cannot open %s", path);
+    CkptHeader h{};
+    if (std::fread(&h, sizeof(h), 1, f) != 1 || std::memcmp(h.magic, "LDAB200", 8) != 0 || h.version != 1) {
+        std::fclose(f);
+        return fail(LDA_ERR_FORMAT, "%s is not a checkpoint of this library", path);
+    }
+    if (h.N != (uint64_t)t->N || h.K != (uint32_t)t->K) {
+        std::fclose(f);
+        return fail(LDA_ERR_FORMAT, "checkpoint holds N=%llu K=%u, trainer has N=%lld K=%d", (unsigned long long)h.N, h.K, (long long)t->N, t->K);
+    }
+    std::vector<uint16_t> z((size_t)t->N);
+    const bool ok = std::fread(z.data(), sizeof(uint16_t), z.size(), f) == z.size();
+    std::fclose(f);
+    if (!ok) return fail(LDA_ERR_FORMAT, "%s is truncated", path);
+    int rc = lda_trainer_set_topics(t, z.data(), t->N);
+    if (rc) return rc;
+    t->seed = h.seed;
+    t->iter = h.iter;
+    return LDA_OK;
+}
+
+// ---------------------------------------------------------------- readback
+
+extern "C" int lda_get_topic_totals(lda_trainer* t, int32_t* nk) {
+    if (!t || !nk) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    CUDA_TRY(cudaMemcpy(nk, t->n_k, sizeof(int) * (size_t)t->K, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}
+
+extern "C" int lda_get_dense_wt(lda_trainer* t, int32_t* out) {
+    if (!t || !out) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    if (t->Vd > 0) CUDA_TRY(cudaMemcpy(out, t->dwt, sizeof(int) * (size_t)t->Vd * t->K, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}
+
+extern "C" int64_t lda_get_sparse_wt(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap) {
+    if (!t || !off) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    const int64_t Vs = t->V - t->Vd;
+    std::vector<uint32_t> hoff(std::max<int64_t>(Vs, 1)), hnnz(std::max<int64_t>(Vs, 1)), hent(std::max<int64_t>(t->swt_cap, 1));
+    if (Vs > 0) {
+        CUDA_TRY(cudaMemcpy(hoff.data(), t->swt_off, sizeof(uint32_t) * (size_t)Vs, cudaMemcpyDeviceToHost));
+        CUDA_TRY(cudaMemcpy(hnnz.data(), t->swt_nnz, sizeof(uint32_t) * (size_t)Vs, cudaMemcpyDeviceToHost));
+    }
+    if (t->swt_cap > 0) CUDA_TRY(cudaMemcpy(hent.data(), t->swt_ent, sizeof(uint32_t) * (size_t)t->swt_cap, cudaMemcpyDeviceToHost));
+    int64_t n = 0;
+    off[0] = 0;
+    for (int64_t s = 0; s < Vs; ++s) {
+        if (ent) {
+            if (n + hnnz[s] > cap) return fail(LDA_ERR_ARG, "sparse WT buffer too small");
+            std::memcpy(ent + n, hent.data() + hoff[s], sizeof(uint32_t) * hnnz[s]);
+        }
+        n += hnnz[s];
+        off[s + 1] = n;
+    }
+    return n;
+}
+
+extern "C" int lda_get_word_stats(lda_trainer* t, uint32_t* top2, uint32_t* k3, float* phi4, float* ql) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    if (top2) CUDA_TRY(cudaMemcpy(top2, t->st_top2, sizeof(uint32_t) * (size_t)t->V, cudaMemcpyDeviceToHost));
+    if (k3) CUDA_TRY(cudaMemcpy(k3, t->st_k3, sizeof(uint32_t) * (size_t)t->V, cudaMemcpyDeviceToHost));
+    if (phi4) CUDA_TRY(cudaMemcpy(phi4, t->st_phi, sizeof(float4) * (size_t)t->V, cudaMemcpyDeviceToHost));
+    if (ql) CUDA_TRY(cudaMemcpy(ql, t->st_ql, sizeof(float) * 32 * (size_t)t->V, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}
+
+extern "C" int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap) {
+    if (!t || !off) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    std::vector<uint32_t> hoff(t->D), hnnz(t->D), hent(std::max<int64_t>(t->dt_cap, 1));
+    CUDA_TRY(cudaMemcpy(hoff.data(), t->dt_off, sizeof(uint32_t) * (size_t)t->D, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hnnz.data(), t->dt_nnz, sizeof(uint32_t) * (size_t)t->D, cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hent.data(), t->dt_ent, sizeof(uint32_t) * (size_t)t->dt_cap, cudaMemcpyDeviceToHost));
+    int64_t n = 0;
+    off[0] = 0;
+    for (int64_t d = 0; d < t->D; ++d) {
+        if (ent) {
+            if (n + hnnz[d] > cap) return fail(LDA_ERR_ARG, "doc-row buffer too small");
+            std::memcpy(ent + n, hent.data() + hoff[d], sizeof(uint32_t) * hnnz[d]);
+        }
+        n += hnnz[d];
+        off[d + 1] = n;
+    }
+    return n;
+}
+
+extern "C" int lda_get_token_meta(lda_trainer* t, uint32_t* meta) {
+    if (!t || !meta) return fail(LDA_ERR_ARG, "null argument");
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    CUDA_TRY(cudaMemcpy(meta, t->meta, sizeof(uint32_t) * (size_t)t->N, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}

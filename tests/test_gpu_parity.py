@@ -1,0 +1,237 @@
+"""GPU parity of the CUDA sweep against the CPU oracle, through the C ABI.
+
+Integer state (n_k, dense/sparse word-topic rows, doc rows, per-token metadata) must be
+bit-exact; per-word float statistics bit-exact; sampled topics identical token for token
+(the kernels and the oracle share one arithmetic specification); the FP64
+log-likelihood within 1e-9 relative (summation order differs)."""
+import os
+
+import numpy as np
+import pytest
+
+import lda_sc20_b200 as L
+from oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+LL_RTOL = 1e-9
+
+
+def _setup(corpus, K, seed=42, nthreads=0):
+    i = corpus.info
+    tr = L.Trainer(corpus, K=K, seed=seed)
+    o = Oracle(corpus.tok_word(), corpus.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, nthreads=nthreads)
+    return tr, o
+
+
+def _compare_state(tr, o, corpus, check_rows=True):
+    i = corpus.info
+    assert np.array_equal(tr.topic_totals(), o.topic_totals())
+    Vd = i.num_dense
+    if Vd:
+        dwt = tr.dense_wt()
+        for w in range(Vd):
+            assert np.array_equal(dwt[w], o.word_row(w)), f"dense word {w}"
+    soff, sent = tr.sparse_wt()
+    ooff, oent = o.word_rows_packed(Vd, i.vocab)
+    assert np.array_equal(soff, ooff)
+    assert np.array_equal(sent, oent)
+    g = tr.word_stats()
+    r = o.word_stats()
+    names = ("top2", "k3", "phi4", "ql")
+    for a, b, n in zip(g, r, names):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
+    if check_rows:
+        goff, gent = tr.doc_rows()
+        roff, rent = o.doc_rows()
+        assert np.array_equal(goff, roff)
+        assert np.array_equal(gent, rent)
+        assert np.array_equal(tr.token_meta(), o.token_meta())
+
+
+@pytest.mark.parametrize("chunks,dense_kind,dense_param", [(1, 0, 0.0), (3, 1, 0.05)])
+def test_stage_parity_one_sweep(chunks, dense_kind, dense_param):
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=chunks, dense_kind=dense_kind, dense_param=dense_param))
+    K = 64
+    tr, o = _setup(c, K)
+    z0 = c.topics()
+    o.rebuild(z0)
+    tr.update_wt()
+    tr.max_topic()
+    for ch in range(c.info.num_chunks):
+        tr.update_dt(ch)
+    tr.sync()
+    _compare_state(tr, o, c)
+    for ch in range(c.info.num_chunks):
+        tr.sample_chunk(ch, ll=True)
+    ll_gpu = tr.perplexity()
+    zo = z0.copy()
+    st = o.sample(zo, 42, 0, ll=True)
+    zg = tr.topics()
+    assert np.array_equal(zg, zo), f"{(zg != zo).sum()} of {len(zo)} topics differ"
+    assert abs(ll_gpu - st.loglik) <= LL_RTOL * abs(st.loglik)
+    cnt = tr.counters()
+    assert cnt.tokens == st.tokens and cnt.early_accept == st.early_accept
+    assert (cnt.branch_max, cnt.branch_s, cnt.branch_q) == (st.branch_max, st.branch_s, st.branch_q)
+
+
+def test_fifty_sweeps_bit_exact_c0():
+    """Config 0 (K=64, ~200K tokens, 50 sweeps): identical topics after every sweep and
+    the LL curve within 1e-9 of the oracle's."""
+    c = L.Corpus.generate(L.corpus_config("c0"))
+    K = 64
+    tr, o = _setup(c, K)
+    z = c.topics()
+    lls = []
+    for it in range(50):
+        st = o.iterate(z, 42, it, ll=True)
+        ll = tr.iterate(1, ll=True)
+        s, n = tr.loglik()
+        assert n == len(z)
+        assert abs(s - st.loglik) <= LL_RTOL * abs(st.loglik), it
+        if it % 5 == 4 or it == 49:
+            zg = tr.topics()
+            assert np.array_equal(zg, z), f"sweep {it}: {(zg != z).sum()} topics differ"
+        lls.append(ll)
+    assert lls[-1] > lls[0]  # the chain is mixing toward higher likelihood
+
+
+@pytest.mark.parametrize("K", [4, 16, 100, 1024])
+def test_k_variants(K):
+    c = L.Corpus.generate(L.corpus_config("c0", num_docs=500, vocab=800, K=K, num_chunks=2))
+    tr, o = _setup(c, K)
+    z = c.topics()
+    for it in range(3):
+        o.iterate(z, 7, it, ll=True)
+    tr2 = L.Trainer(c, K=K, seed=7)
+    tr2.iterate(3, ll=True)
+    assert np.array_equal(tr2.topics(), z)
+    del tr
+
+
+def test_mid_size_k1024_lognormal():
+    cfg = L.corpus_config("c1", num_docs=20000, vocab=20000, num_chunks=4, corpus_seed=77)
+    c = L.Corpus.generate(cfg)
+    K = 1024
+    tr, o = _setup(c, K)
+    z = c.topics()
+    for it in range(3):
+        st = o.iterate(z, 42, it, ll=True)
+        tr.iterate(1, ll=True)
+        s, _ = tr.loglik()
+        assert abs(s - st.loglik) <= LL_RTOL * abs(st.loglik)
+    assert np.array_equal(tr.topics(), z)
+    o.rebuild(z)
+    tr.update_wt()
+    tr.max_topic()
+    for ch in range(c.info.num_chunks):
+        tr.update_dt(ch)
+    tr.sync()
+    _compare_state(tr, o, c)
+
+
+def test_empty_docs_and_tiny_corpus():
+    rng = np.random.default_rng(1)
+    lens = rng.integers(0, 30, size=64)
+    lens[[0, 7, 63]] = 0
+    off = np.concatenate([[0], np.cumsum(lens)])
+    words = rng.integers(0, 40, size=off[-1]).astype(np.int32)
+    c = L.Corpus.from_docs(off, words, vocab=40, K=8, num_chunks=3)
+    tr, o = _setup(c, 8)
+    z = c.topics()
+    for it in range(4):
+        o.iterate(z, 42, it)
+        tr.iterate(1)
+    assert np.array_equal(tr.topics(), z)
+
+
+def test_host_iterate_matches_resident():
+    c = L.Corpus.generate(L.corpus_config("c0"))
+    a = L.Trainer(c, K=64)
+    b = L.Trainer(c, K=64)
+    z = c.topics()
+    out = np.empty_like(z)
+    for it in range(3):
+        lb = b.iterate_host(z, out, ll=True)
+        a.iterate(1, ll=True)
+        z = out.copy()
+        assert abs(a.loglik()[0] - lb) <= 1e-12 * abs(lb)
+    assert np.array_equal(a.topics(), out)
+
+
+def test_checkpoint_resume_is_exact(tmp_path):
+    c = L.Corpus.generate(L.corpus_config("c0"))
+    a = L.Trainer(c, K=64)
+    a.iterate(5)
+    p = str(tmp_path / "ck.bin")
+    a.checkpoint(p)
+    a.iterate(5)
+    b = L.Trainer(c, K=64, seed=999)
+    b.restore(p)
+    assert b.iteration == 5
+    b.iterate(5)
+    assert np.array_equal(a.topics(), b.topics())
+
+
+def test_device_budget_and_topic_validation():
+    c = L.Corpus.generate(L.corpus_config("c0"))
+    with pytest.raises(L.LdaError) as e:
+        L.Trainer(c, K=64, device_budget=1 << 16)
+    assert e.value.code == -5  # LDA_ERR_DEVICE_MEM
+    tr = L.Trainer(c, K=64)
+    bad = c.topics()
+    bad[3] = 64
+    with pytest.raises(L.LdaError) as e:
+        tr.set_topics(bad)
+    assert e.value.code == -1
+    with pytest.raises(L.LdaError) as e:
+        tr.perplexity()  # no chunk sampled with ll
+    assert e.value.code == -7
+
+
+def _row_sums(off, ent):
+    rows = np.repeat(np.arange(len(off) - 1), np.diff(off))
+    return np.bincount(rows, weights=(ent & 0xFFFF).astype(np.float64), minlength=len(off) - 1).astype(np.int64)
+
+
+@pytest.mark.slow
+def test_config1_full_size_properties():
+    """Config 1 at full size (K=1024, ~72M tokens): count invariants, determinism, and
+    token-for-token agreement with the oracle on every 97th word."""
+    c = L.Corpus.generate(L.corpus_config("c1"))
+    i = c.info
+    K = 1024
+    tr = L.Trainer(c, K=K)
+    z0 = c.topics()
+    tr.update_wt()
+    tr.max_topic()
+    for ch in range(i.num_chunks):
+        tr.update_dt(ch)
+    tr.sync()
+    nk = tr.topic_totals()
+    assert nk.sum() == i.num_tokens and np.array_equal(nk, np.bincount(z0, minlength=K))
+    wc = c.word_count()
+    assert np.array_equal(tr.dense_wt().sum(1), wc[: i.num_dense])
+    soff, sent = tr.sparse_wt()
+    assert np.array_equal(_row_sums(soff, sent), wc[i.num_dense:])
+    goff, gent = tr.doc_rows()
+    assert np.array_equal(_row_sums(goff, gent), np.diff(c.doc_off()))
+    for ch in range(i.num_chunks):
+        tr.sample_chunk(ch, ll=True)
+    ll = tr.perplexity()
+    tr.end_sweep()
+    z1 = tr.topics()
+    assert np.isfinite(ll) and z1.max() < K
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta)
+    o.rebuild(z0)
+    zo = z0.copy()
+    st = o.sample(zo, 42, 0, word_stride=97)
+    tw = c.tok_word()
+    sel = (tw % 97) == 0
+    assert st.tokens == sel.sum()
+    assert np.array_equal(z1[sel], zo[sel])
+    # determinism: a second trainer reproduces the sweep exactly
+    tr2 = L.Trainer(c, K=K)
+    tr2.iterate(1, ll=True)
+    assert np.array_equal(tr2.topics(), z1)
+    assert tr2.loglik()[0] == ll
