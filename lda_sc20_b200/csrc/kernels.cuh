@@ -316,13 +316,16 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
 }
 
 // ------------------------------------------------------------------- sampler
-// Warp per (word, token range) tile.  The word's phi column (with phi_max zeroed) sits in
-// warp-private shared memory.  Each 32-token group is first screened thread-per-token by
-// the max-topic bound; tokens that fail it (all tokens in LL mode) are then evaluated one
-// at a time by the whole warp: 4-entry vector loads of the doc row, per-lane partial S,
-// one Kogge-Stone scan, ballot bin search, single-lane refinement.  Replaces
-// UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain (EZLDA/utility.cu:2680-3312,
-// :1625-2103, :1217-1611) in one pass, with no effective-token list and no spin lock.
+// Warp per (word, token range) tile; thread per token.  The word's phi column (phi_max
+// zeroed) and the lane prefix of its Q bucket sit in warp-private shared memory.  Each
+// lane takes one token of a 32-token group: Philox u, the max-topic bound (early accept),
+// and, for tokens the bound does not settle (all tokens in LL mode), the full
+// conditional: S as a serial sum over the doc row (16-byte vector loads), then the
+// three-way branch and the bin search (serial over the row for the S bucket; lane prefix
+// then the lane's topics for the Q bucket).  32 tokens are in flight per warp, so the
+// doc-row loads of a warp overlap.  Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and
+// LDAKernelTrain (EZLDA/utility.cu:2680-3312, :1625-2103, :1217-1611) in one pass, with
+// no effective-token list and no spin lock.
 struct SampleArgs {
     const int4* tiles;  // {word, start, count, dense}
     int ntiles;
@@ -350,11 +353,55 @@ struct SampleArgs {
     unsigned long long* ctr;  // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles
 };
 
+// S = serial sum over the doc row (ascending k) of count * colz[k].
+__device__ __forceinline__ float row_mass(const uint32_t* __restrict__ row, uint32_t nnz, const float* col) {
+    float S = 0.0f;
+    uint32_t q = 0;
+    for (; q + 4 <= nnz; q += 4) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
+        S = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], S);
+        S = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], S);
+        S = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], S);
+        S = ffma(u2f(v.w & 0xffffu), col[v.w >> 16], S);
+    }
+    if (q < nnz) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
+        S = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], S);
+        if (q + 1 < nnz) S = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], S);
+        if (q + 2 < nnz) S = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], S);
+    }
+    return S;
+}
+
+// First row entry with colz > 0 whose running sum exceeds t (else the last such entry).
+__device__ __forceinline__ int row_search(const uint32_t* __restrict__ row, uint32_t nnz, const float* col, float t) {
+    float acc = 0.0f;
+    int last = -1;
+    for (uint32_t q = 0; q < nnz; q += 4) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
+        const uint32_t e4[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            if (q + i < nnz) {
+                const uint32_t k = e4[i] >> 16;
+                const float cz = col[k];
+                acc = ffma(u2f(e4[i] & 0xffffu), cz, acc);
+                if (cz > 0.0f) {
+                    last = (int)k;
+                    if (t < acc) return (int)k;
+                }
+            }
+        }
+    }
+    return last;
+}
+
 __global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
     extern __shared__ float smf[];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* r = smf;
     float* col = smf + (size_t)a.K * (1 + wid);
+    float* qlp = smf + (size_t)a.K * (1 + warps) + 64 * wid;  // [0,32): QL, [32,64): QP
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     __syncthreads();
     uint32_t c_tok = 0, c_ea = 0, c_full = 0, c_nnz = 0, c_max = 0, c_s = 0, c_q = 0, c_wnnz = 0;
@@ -378,102 +425,60 @@ __global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
         const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
         const float QP = warp_ks_scan(QL, lane);
         const float Q = __shfl_sync(FULL, QP, 31);
+        qlp[lane] = QL;
+        qlp[32 + lane] = QP;
         if (lane == 0) col[maxK] = 0.0f;
         __syncwarp();
         double ll = 0.0;
         for (uint32_t g = 0; g < cnt; g += 32) {
-            const bool valid = g + lane < cnt;
+            if (g + lane >= cnt) continue;
             const uint32_t tok = start + g + lane;
-            uint32_t d = 0, nd = 0;
-            float u = 0.0f, pmax = 0.0f;
-            bool ea = false;
-            if (valid) {
-                d = __ldg(a.tok_doc + tok);
-                const uint32_t m = __ldg(a.meta + tok);
-                nd = __ldg(a.doc_len + d);
-                const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
-                u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
-                pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
-                const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
-                const float bound = fadd(fadd(pmax, shat), Q);
-                ea = fmul(u, bound) < pmax;
-                c_tok++;
-                c_ea += ea;
-            }
+            const uint32_t d = __ldg(a.tok_doc + tok);
+            const uint32_t m = __ldg(a.meta + tok);
+            const uint32_t nd = __ldg(a.doc_len + d);
+            const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
+            const float u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
+            const float pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
+            const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
+            const float bound = fadd(fadd(pmax, shat), Q);
+            const bool ea = fmul(u, bound) < pmax;
+            c_tok++;
+            c_ea += ea;
             int znew = maxK;
-            unsigned need = __ballot_sync(FULL, valid && (!ea || a.ll_mode));
-            while (need) {
-                const int j = __ffs(need) - 1;
-                need &= need - 1u;
-                const uint32_t dj = __shfl_sync(FULL, d, j);
-                const uint32_t ndj = __shfl_sync(FULL, nd, j);
-                const float pmj = __shfl_sync(FULL, pmax, j);
-                const float uj = __shfl_sync(FULL, u, j);
-                const int eaj = __shfl_sync(FULL, (int)ea, j);
-                const uint32_t nnz = __ldg(a.dt_nnz + dj);
-                const uint32_t* row = a.dt_ent + __ldg(a.dt_off + dj);
-                float SL = 0.0f;
-                for (uint32_t q = 4u * lane; q < nnz; q += 128u) {
-                    const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
-                    SL = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], SL);
-                    if (q + 1 < nnz) SL = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], SL);
-                    if (q + 2 < nnz) SL = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], SL);
-                    if (q + 3 < nnz) SL = ffma(u2f(v.w & 0xffffu), col[v.w >> 16], SL);
-                }
-                const float SP = warp_ks_scan(SL, lane);
-                const float S = __shfl_sync(FULL, SP, 31);
-                const float pS = fadd(pmj, S);
+            if (!ea || a.ll_mode) {
+                const uint32_t nnz = __ldg(a.dt_nnz + d);
+                const uint32_t* row = a.dt_ent + __ldg(a.dt_off + d);
+                const float S = row_mass(row, nnz, col);
+                const float pS = fadd(pmax, S);
                 const float total = fadd(pS, Q);
-                if (lane == 0) {
-                    c_full++;
-                    c_nnz += nnz;
-                }
-                if (a.ll_mode && lane == j) ll += log((double)total / ((double)ndj + a.den_add));
-                if (!eaj) {
-                    const float target = fmul(uj, total);
-                    int zj;
-                    if (target < pmj) {
-                        zj = maxK;
-                        c_max += (lane == 0);
+                c_full++;
+                c_nnz += nnz;
+                if (a.ll_mode) ll += log((double)total / ((double)nd + a.den_add));
+                if (!ea) {
+                    const float target = fmul(u, total);
+                    if (target < pmax) {
+                        c_max++;
                     } else if (target < pS) {
-                        const float tt = fsub(target, pmj);
-                        const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
-                        const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
-                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
-                        const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
-                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
-                        int found = -1, last = -1;
-                        if (lane == ls) {
-                            float acc = 0.0f;
-                            for (uint32_t q = 4u * ls; q < nnz && found < 0; q += 128u) {
-                                const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
-                                const uint32_t e4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-                                for (int i = 0; i < 4; ++i) {
-                                    if (q + i < nnz && found < 0) {
-                                        const uint32_t k = e4[i] >> 16;
-                                        const float cz = col[k];
-                                        acc = ffma(u2f(e4[i] & 0xffffu), cz, acc);
-                                        if (cz > 0.0f) {
-                                            last = (int)k;
-                                            if (t2 < acc) found = (int)k;
-                                        }
-                                    }
+                        const int k = row_search(row, nnz, col, fsub(target, pmax));
+                        znew = k >= 0 ? k : maxK;
+                        c_s++;
+                    } else {
+                        const float tt = fsub(target, pS);
+                        int ls = -1, lastpos = -1;
+                        for (int l = 0; l < 32; ++l) {
+                            const float ql = qlp[l];
+                            if (ql > 0.0f) {
+                                lastpos = l;
+                                if (tt < qlp[32 + l]) {
+                                    ls = l;
+                                    break;
                                 }
                             }
                         }
-                        zj = __shfl_sync(FULL, found >= 0 ? found : last, ls & 31);
-                        if (ls < 0 || zj < 0) zj = maxK;
-                        c_s += (lane == 0);
-                    } else {
-                        const float tt = fsub(target, pS);
-                        const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
-                        const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
-                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
-                        const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
-                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                        if (ls < 0) ls = lastpos;
                         int found = -1, last = -1;
-                        if (lane == ls) {
+                        if (ls >= 0) {
+                            const float t2 = ls > 0 ? fsub(tt, qlp[32 + ls - 1]) : tt;
                             float acc = 0.0f;
                             for (int k = ls; k < a.K; k += 32) {
                                 const float cz = col[k];
@@ -487,19 +492,16 @@ __global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
                                 }
                             }
                         }
-                        zj = __shfl_sync(FULL, found >= 0 ? found : last, ls & 31);
-                        if (ls < 0 || zj < 0) zj = maxK;
-                        c_q += (lane == 0);
+                        znew = found >= 0 ? found : (last >= 0 ? last : maxK);
+                        c_q++;
                     }
-                    if (lane == j) znew = zj;
                 } else {
-                    c_max += (lane == 0);
+                    c_max++;
                 }
+            } else {
+                c_max++;
             }
-            if (valid) {
-                if (ea && !a.ll_mode) c_max++;
-                a.z[tok] = (uint16_t)znew;
-            }
+            a.z[tok] = (uint16_t)znew;
         }
         if (a.ll_mode) {
 #pragma unroll

@@ -188,9 +188,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     T.chunk_doc = c->chunk_doc;
     // warps per CTA: (warps + 1) K-wide shared rows must fit
     const int64_t row = (int64_t)T.K * 4;
-    T.warps = (int)std::min<int64_t>(8, (int64_t)max_smem / row - 1);
+    T.warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
-    T.smem_wt = T.smem_stats = T.smem_sample = (size_t)(T.warps + 1) * row;
+    T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
+    T.smem_sample = (size_t)(T.warps + 1) * row + (size_t)T.warps * 64 * sizeof(float);
     T.smem_dt = (size_t)T.warps * row;
 
     // ---- host-side derived layout

@@ -35,15 +35,18 @@
  *   shat    = fmaf((float)c2, phi_2nd, (float)rest * phi_3rd)
  *   bound   = (pmax + shat) + Q;   early accept  <=>  u*bound < pmax
  *   colz    = phi with colz[maxK] = 0
- *   SL[l]   = serial fmaf((float)cnt_e, colz[k_e], acc) over doc-row entries
- *             e = 128r + 4l + i (r = 0,1,..; i = 0..3; e < nnz)
- *   SP      = Kogge-Stone scan of SL; S = SP[31]
+ *   S       = serial fmaf((float)cnt_e, colz[k_e], acc) over the doc row in
+ *             ascending k (e = 0..nnz-1)
  *   pS      = pmax + S; total = pS + Q; target = u*total
- *   target < pmax -> maxK; target < pS -> S bucket (t = target - pmax);
- *   else Q bucket (t = target - pS).  Bucket search: first lane l with
- *   t < P[l] and L[l] > 0 (else the last lane with L[l] > 0), then
- *   t2 = t - P[l-1] and the first owned entry whose serial partial sum exceeds
- *   t2 (else the last owned entry with colz > 0).
+ *   target < pmax -> maxK;
+ *   target < pS   -> S bucket: t = target - pmax; the first row entry with
+ *                    colz > 0 whose running sum (same serial fmaf) exceeds t,
+ *                    else the last row entry with colz > 0;
+ *   otherwise     -> Q bucket: t = target - pS; the first lane l with t < QP[l]
+ *                    and QL[l] > 0 (else the last lane with QL[l] > 0), then
+ *                    t2 = t - QP[l-1] and the first k = l, l+32, ... with
+ *                    colz > 0 whose serial fmaf(alpha, colz[k], acc) exceeds t2
+ *                    (else the last such k).
  *   LL_i    = log((double)total / ((double)n_d + (double)K * (double)alpha))
  * Randoms: u = (float)(x0 >> 8) * 2^-24 with x = Philox4x32-10(ctr = {tok_lo,
  * tok_hi, iter, 0x4C444131}, key = {seed_lo, seed_hi}); initial topic =
@@ -515,15 +518,10 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
             st->tokens++;
             if (ea) st->early_accept++;
             if (ea && !x->ll_mode) { x->z_out[t] = (uint16_t)maxK; st->branch_max++; continue; }
-            /* S over the doc row, lane-strided by 4-entry vectors */
-            float SL[LANES], SP[LANES];
-            memset(SL, 0, sizeof(SL));
-            for (int32_t q = 0; q < nnz; ++q) {
-                int l = (q >> 2) & (LANES - 1);
-                SL[l] = fmaf((float)(row[q] & 0xffffu), colz[row[q] >> 16], SL[l]);
-            }
-            ks_scan32(SL, SP);
-            const float S = SP[LANES - 1];
+            /* S: serial sum over the doc row in ascending k (EZLDA/utility.cu:1376-1440
+             * sums the same row in 32-entry blocks) */
+            float S = 0.0f;
+            for (int32_t q = 0; q < nnz; ++q) S = fmaf((float)(row[q] & 0xffffu), colz[row[q] >> 16], S);
             const float pS = pmax + S;
             const float total = pS + Q;
             st->full++;
@@ -536,22 +534,17 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
                 znew = maxK;
                 st->branch_max++;
             } else if (target < pS) {
+                /* first row entry with colz > 0 whose running sum exceeds t */
                 const float tt = target - pmax;
-                int l = pick_lane(tt, SP, SL);
-                float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
                 float acc = 0.0f;
                 int32_t found = -1, last = -1;
-                for (int32_t q = 4 * l; l >= 0 && q < nnz; q += 4 * LANES) {
-                    for (int32_t i = 0; i < 4 && q + i < nnz; ++i) {
-                        uint32_t en = row[q + i];
-                        int32_t k = (int32_t)(en >> 16);
-                        acc = fmaf((float)(en & 0xffffu), colz[k], acc);
-                        if (colz[k] > 0.0f) {
-                            last = k;
-                            if (t2 < acc) { found = k; break; }
-                        }
+                for (int32_t q = 0; q < nnz; ++q) {
+                    const int32_t k = (int32_t)(row[q] >> 16);
+                    acc = fmaf((float)(row[q] & 0xffffu), colz[k], acc);
+                    if (colz[k] > 0.0f) {
+                        last = k;
+                        if (tt < acc) { found = k; break; }
                     }
-                    if (found >= 0) break;
                 }
                 znew = found >= 0 ? found : last;
                 if (znew < 0) znew = maxK; /* no positive bin (cannot happen for beta > 0) */
