@@ -219,6 +219,56 @@ int lda_get_word_stats(lda_trainer* t, uint32_t* top2, uint32_t* k3, float* phi4
 int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap);
 int lda_get_token_meta(lda_trainer* t, uint32_t* meta /*N*/);
 
+/* ------------------------------------------------ allocation-free sampling */
+
+/* Device buffers of one sampling call (all device pointers; sizes implied by the
+ * corpus layout): tiles is num_tiles x {word, first token, token count, dense flag}
+ * (16-byte aligned); the rest follow the layout lda_get_* return, with every doc row
+ * starting at a multiple of 4 entries of dt_ent (16-byte aligned rows). */
+typedef struct {
+    int32_t K, num_dense, vocab;
+    float alpha, beta;
+    uint64_t seed;
+    uint32_t iter;
+    int32_t ll_mode;
+    int32_t num_tiles;
+    const int32_t* tiles;
+    const int32_t* n_k;            /* [K] */
+    const int32_t* dense_wt;       /* [num_dense*K] */
+    const uint32_t* sparse_off;    /* [vocab-num_dense] */
+    const uint32_t* sparse_nnz;    /* [vocab-num_dense] */
+    const uint32_t* sparse_ent;    /* (k<<16 | count) */
+    const uint32_t* top2;          /* [vocab] */
+    const float* phi4;             /* [vocab*4] */
+    const float* ql;               /* [vocab*32] */
+    const uint32_t* tok_doc;       /* [N] */
+    const uint32_t* meta;          /* [N] */
+    uint16_t* topics;              /* [N], updated for the tiles' tokens */
+    const uint32_t* doc_len;       /* [D] */
+    const uint32_t* dt_off;        /* [D] */
+    const uint32_t* dt_nnz;        /* [D] */
+    const uint32_t* dt_ent;
+    double* ll_sum;                /* device scalar, written when ll_mode */
+} lda_sample_io;
+
+/* Samples the tokens of io->tiles exactly as lda_sample_chunk does, but allocates
+ * nothing: no cudaMalloc, cudaFree or allocating library call.  It exists for callers
+ * that own all device memory through their own allocator or a pre-reserved arena (a
+ * serving process that has handed HBM to its pool, an embedding framework with its own
+ * caching allocator), where a library-side cudaMalloc/cudaFree would synchronise the
+ * device, fragment the pool, or fail with out-of-memory in the middle of a request.
+ * No counterpart in the reference: EZLDA allocates everything up front in its classes.
+ *
+ * Its scratch (tile counter, sweep counters, per-tile LL partials) is one file-scope
+ * device array of 524,544 bytes that every GPU loading the library holds until the
+ * process exits.  Limits: num_tiles <= 65536 (LDA_ERR_ARG beyond), K <= the largest K a
+ * trainer accepts.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress with that device current); make that first call before any
+ * stream capture.  Every call shares the array, so calls that overlap on the GPU (on
+ * different streams or devices sharing a context) race; serialise them.  The call is
+ * asynchronous on `stream` (NULL: the legacy default stream) and sets `device` current. */
+int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

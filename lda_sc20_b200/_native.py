@@ -61,6 +61,20 @@ class StageTiming(C.Structure):
                                          "launches_sample", "launches_ll")]
 
 
+class SampleIO(C.Structure):
+    """lda_sample_io: device buffers of one allocation-free sampling call."""
+    _fields_ = [
+        ("K", C.c_int32), ("num_dense", C.c_int32), ("vocab", C.c_int32),
+        ("alpha", C.c_float), ("beta", C.c_float), ("seed", C.c_uint64), ("iter", C.c_uint32),
+        ("ll_mode", C.c_int32), ("num_tiles", C.c_int32),
+        ("tiles", C.c_void_p), ("n_k", C.c_void_p), ("dense_wt", C.c_void_p), ("sparse_off", C.c_void_p),
+        ("sparse_nnz", C.c_void_p), ("sparse_ent", C.c_void_p), ("top2", C.c_void_p), ("phi4", C.c_void_p),
+        ("ql", C.c_void_p), ("tok_doc", C.c_void_p), ("meta", C.c_void_p), ("topics", C.c_void_p),
+        ("doc_len", C.c_void_p), ("dt_off", C.c_void_p), ("dt_nnz", C.c_void_p), ("dt_ent", C.c_void_p),
+        ("ll_sum", C.c_void_p),
+    ]
+
+
 P = C.c_void_p
 I32, I64, U32, U64, F32, F64 = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_float, C.c_double
 
@@ -107,6 +121,7 @@ SIGNATURES = {
     "lda_get_word_stats": (I32, [P, P, P, P, P]),
     "lda_get_doc_rows": (I64, [P, P, P, I64]),
     "lda_get_token_meta": (I32, [P, P]),
+    "lda_sample_chunk_noalloc": (I32, [C.POINTER(SampleIO), I32, P]),
 }
 
 _lib = None

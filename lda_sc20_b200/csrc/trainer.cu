@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -718,5 +719,103 @@ extern "C" int lda_get_token_meta(lda_trainer* t, uint32_t* meta) {
     CUDA_TRY(cudaSetDevice(t->device));
     CUDA_TRY(cudaStreamSynchronize(t->stream));
     CUDA_TRY(cudaMemcpy(meta, t->meta, sizeof(uint32_t) * (size_t)t->N, cudaMemcpyDeviceToHost));
+    return LDA_OK;
+}
+
+// ------------------------------------------------------- allocation-free sampling
+//
+// lda_sample_chunk_noalloc runs the same k_sample / k_ll_reduce kernels on buffers the
+// caller owns.  Its scratch lives in one file-scope device array: bytes [0,4) the tile
+// counter, [8,136) the sweep counters, [256, 256 + 8*kNoAllocMaxTiles) the per-tile LL
+// partials.  In host code the symbol is only a host-side stand-in, so the device address
+// is looked up once per device (with that device current) and cached.
+
+namespace {
+constexpr int kNoAllocMaxTiles = 65536;
+constexpr size_t kNoAllocHeader = 256;
+constexpr size_t kNoAllocBytes = kNoAllocHeader + sizeof(double) * (size_t)kNoAllocMaxTiles;
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned char* g_noalloc_addr[kMaxDevices] = {};
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+static int noalloc_scratch(int device, unsigned char** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(LDA_ERR_ARG, "device %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));  // `device` is current here
+        g_noalloc_addr[device] = (unsigned char*)p;
+    }
+    *out = g_noalloc_addr[device];
+    return LDA_OK;
+}
+
+extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream_ptr) {
+    if (!io) return fail(LDA_ERR_ARG, "null io");
+    if (io->K < 4 || io->K > 65535) return fail(LDA_ERR_ARG, "K=%d outside [4, 65535]", io->K);
+    if (io->num_tiles < 0 || io->num_tiles > kNoAllocMaxTiles)
+        return fail(LDA_ERR_ARG, "num_tiles=%d exceeds the allocation-free limit of %d tiles per call",
+                    io->num_tiles, kNoAllocMaxTiles);
+    if (io->vocab <= 0 || io->num_dense < 0 || io->num_dense > io->vocab)
+        return fail(LDA_ERR_ARG, "bad vocab / num_dense");
+    if (!(io->alpha > 0.f) || !(io->beta > 0.f)) return fail(LDA_ERR_ARG, "alpha and beta must be > 0");
+    if (io->num_tiles > 0 &&
+        (!io->tiles || !io->n_k || !io->top2 || !io->phi4 || !io->ql || !io->tok_doc || !io->meta || !io->topics ||
+         !io->doc_len || !io->dt_off || !io->dt_nnz || !io->dt_ent || (io->num_dense > 0 && !io->dense_wt) ||
+         (io->num_dense < io->vocab && (!io->sparse_off || !io->sparse_nnz || !io->sparse_ent)) ||
+         (io->ll_mode && !io->ll_sum)))
+        return fail(LDA_ERR_ARG, "null device buffer in lda_sample_io");
+    if (((uintptr_t)io->tiles & 15u) || ((uintptr_t)io->dt_ent & 15u) || ((uintptr_t)io->phi4 & 15u))
+        return fail(LDA_ERR_ARG, "tiles, phi4 and dt_ent must be 16-byte aligned");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        cudaGetLastError();
+        return fail(LDA_ERR_CUDA, "CUDA device %d not available", device);
+    }
+    CUDA_TRY(cudaSetDevice(device));
+    unsigned char* scratch = nullptr;
+    int rc = noalloc_scratch(device, &scratch);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream_ptr;
+    CUDA_TRY(cudaMemsetAsync(scratch, 0, kNoAllocHeader, st));  // tile counter + sweep counters
+    if (io->num_tiles == 0) {
+        if (io->ll_mode) CUDA_TRY(cudaMemsetAsync(io->ll_sum, 0, sizeof(double), st));
+        return LDA_OK;
+    }
+    int max_smem = 0, num_sms = 0;
+    CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
+    CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
+    const int64_t row = (int64_t)io->K * 4;
+    const int warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
+    if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
+    const size_t smem = (size_t)(warps + 1) * row + (size_t)warps * 64 * sizeof(float);
+    CUDA_TRY(cudaFuncSetAttribute((const void*)dev::k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int grid = 0;
+    if ((rc = occupancy_grid((const void*)dev::k_sample, 32 * warps, smem, num_sms, &grid))) return rc;
+    grid = std::max(1, std::min(grid, (io->num_tiles + warps - 1) / warps));
+    dev::SampleArgs a;
+    a.tiles = reinterpret_cast<const int4*>(io->tiles);
+    a.ntiles = io->num_tiles;
+    a.tile_counter = reinterpret_cast<unsigned*>(scratch);
+    a.tile_ll = reinterpret_cast<double*>(scratch + kNoAllocHeader);
+    a.K = io->K; a.Vd = io->num_dense; a.ll_mode = io->ll_mode ? 1 : 0;
+    a.alpha = io->alpha; a.beta = io->beta; a.Vbeta = (float)io->vocab * io->beta;
+    a.den_add = (double)io->K * (double)io->alpha;
+    a.seed_lo = (uint32_t)io->seed; a.seed_hi = (uint32_t)(io->seed >> 32); a.iter = io->iter;
+    a.n_k = io->n_k; a.dwt = io->dense_wt;
+    a.swt_off = io->sparse_off; a.swt_nnz = io->sparse_nnz; a.swt_ent = io->sparse_ent;
+    a.st_top2 = io->top2; a.st_phi = reinterpret_cast<const float4*>(io->phi4); a.st_ql = io->ql;
+    a.tok_doc = io->tok_doc; a.meta = io->meta; a.z = io->topics; a.doc_len = io->doc_len;
+    a.dt_off = io->dt_off; a.dt_nnz = io->dt_nnz; a.dt_ent = io->dt_ent;
+    a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
+    dev::k_sample<<<grid, 32 * warps, smem, st>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    if (io->ll_mode) {
+        dev::k_ll_reduce<<<1, 1024, 0, st>>>(a.tile_ll, io->num_tiles, io->ll_sum);
+        CUDA_TRY(cudaGetLastError());
+    }
     return LDA_OK;
 }
