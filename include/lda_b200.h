@@ -130,6 +130,8 @@ typedef struct {
     int64_t branch_max, branch_s, branch_q;
     int64_t sum_word_nnz;  /* sparse word-row entries read building word columns */
     int64_t word_tiles_dense, word_tiles_sparse;
+    int64_t rows_evaluated;   /* doc rows evaluated (consecutive tokens of one (word, doc) share one) */
+    int64_t row_entries_read; /* doc-row entries read by those evaluations */
 } lda_sweep_counters;
 
 /* Accumulated device time (CUDA events on the trainer's stream) per stage. */

@@ -158,6 +158,8 @@ class SweepStats:
     sum_word_nnz: int
     word_tiles_dense: int
     word_tiles_sparse: int
+    rows_evaluated: int
+    row_entries_read: int
 
 
 class Trainer:
@@ -238,7 +240,8 @@ class Trainer:
         c = SweepCounters()
         check(self._lib.lda_trainer_counters(self._h, C.byref(c)))
         return SweepStats(c.tokens, c.early_accept, c.full, c.sum_nnz_full, c.branch_max, c.branch_s,
-                          c.branch_q, c.sum_word_nnz, c.word_tiles_dense, c.word_tiles_sparse)
+                          c.branch_q, c.sum_word_nnz, c.word_tiles_dense, c.word_tiles_sparse,
+                          c.rows_evaluated, c.row_entries_read)
 
     def set_timing(self, on: bool) -> None:
         check(self._lib.lda_trainer_set_timing(self._h, 1 if on else 0))

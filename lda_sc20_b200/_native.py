@@ -52,7 +52,7 @@ class TrainConfig(C.Structure):
 class SweepCounters(C.Structure):
     _fields_ = [(n, C.c_int64) for n in (
         "tokens", "early_accept", "full", "sum_nnz_full", "branch_max", "branch_s", "branch_q",
-        "sum_word_nnz", "word_tiles_dense", "word_tiles_sparse")]
+        "sum_word_nnz", "word_tiles_dense", "word_tiles_sparse", "rows_evaluated", "row_entries_read")]
 
 
 class StageTiming(C.Structure):

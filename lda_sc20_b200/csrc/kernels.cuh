@@ -316,16 +316,21 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
 }
 
 // ------------------------------------------------------------------- sampler
-// Warp per (word, token range) tile; thread per token.  The word's phi column (phi_max
-// zeroed) and the lane prefix of its Q bucket sit in warp-private shared memory.  Each
-// lane takes one token of a 32-token group: Philox u, the max-topic bound (early accept),
-// and, for tokens the bound does not settle (all tokens in LL mode), the full
-// conditional: S as a serial sum over the doc row (16-byte vector loads), then the
-// three-way branch and the bin search (serial over the row for the S bucket; lane prefix
-// then the lane's topics for the Q bucket).  32 tokens are in flight per warp, so the
-// doc-row loads of a warp overlap.  Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and
-// LDAKernelTrain (EZLDA/utility.cu:2680-3312, :1625-2103, :1217-1611) in one pass, with
-// no effective-token list and no spin lock.
+// Warp per (word, token range) tile.  The word's phi column (phi_max zeroed) sits in
+// warp-private shared memory.  Each 32-token group is screened thread-per-token by the
+// max-topic bound.  Tokens the bound does not settle (all tokens in LL mode) are then
+// evaluated one at a time by the whole warp, with uniform control flow:
+//   S      lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
+//          one Kogge-Stone scan gives the lane prefixes; a doc row is evaluated once
+//          for consecutive tokens of the same (word, doc) in the tile;
+//   search ballot over the lane prefixes picks the block, then each lane takes one
+//          entry of it and a second scan plus a ballot pick the topic (32 entries per
+//          round, carried across rounds);
+//   Q      the same two levels over the per-word lane prefixes of Q and the lane's
+//          topics k = l, l+32, ...
+// Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain
+// (EZLDA/utility.cu:2680-3312, :1625-2103, :1217-1611) in one pass, with no
+// effective-token list in global memory and no spin lock.
 struct SampleArgs {
     const int4* tiles;  // {word, start, count, dense}
     int ntiles;
@@ -350,62 +355,41 @@ struct SampleArgs {
     const uint32_t* dt_off;
     const uint32_t* dt_nnz;
     const uint32_t* dt_ent;
-    unsigned long long* ctr;  // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles
+    // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles, rows, row entries
+    unsigned long long* ctr;
 };
 
-// S = serial sum over the doc row (ascending k) of count * colz[k].
-__device__ __forceinline__ float row_mass(const uint32_t* __restrict__ row, uint32_t nnz, const float* col) {
-    float S = 0.0f;
-    uint32_t q = 0;
-    for (; q + 4 <= nnz; q += 4) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
-        S = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], S);
-        S = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], S);
-        S = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], S);
-        S = ffma(u2f(v.w & 0xffffu), col[v.w >> 16], S);
-    }
-    if (q < nnz) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
-        S = ffma(u2f(v.x & 0xffffu), col[v.x >> 16], S);
-        if (q + 1 < nnz) S = ffma(u2f(v.y & 0xffffu), col[v.y >> 16], S);
-        if (q + 2 < nnz) S = ffma(u2f(v.z & 0xffffu), col[v.z >> 16], S);
-    }
-    return S;
-}
-
-// First row entry with colz > 0 whose running sum exceeds t (else the last such entry).
-__device__ __forceinline__ int row_search(const uint32_t* __restrict__ row, uint32_t nnz, const float* col, float t) {
-    float acc = 0.0f;
+// Second-level search over 32-entry rounds: term = weight of slot i, ok = slot may be
+// drawn; returns the key of the first ok slot whose carried scan exceeds t2, else the
+// last ok slot's key, else `fallback`.  Uniform across the warp.
+template <class Slot>
+__device__ __forceinline__ int warp_level2(uint32_t n, float t2, int fallback, int lane, Slot slot) {
+    float carry = 0.0f;
     int last = -1;
-    for (uint32_t q = 0; q < nnz; q += 4) {
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + q));
-        const uint32_t e4[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            if (q + i < nnz) {
-                const uint32_t k = e4[i] >> 16;
-                const float cz = col[k];
-                acc = ffma(u2f(e4[i] & 0xffffu), cz, acc);
-                if (cz > 0.0f) {
-                    last = (int)k;
-                    if (t < acc) return (int)k;
-                }
-            }
-        }
+    for (uint32_t base = 0; base < n; base += 32) {
+        int key = -1;
+        float term = 0.0f;
+        bool ok = false;
+        if (base + lane < n) slot(base + lane, key, term, ok);
+        const float P = fadd(carry, warp_ks_scan(term, lane));
+        const unsigned f = __ballot_sync(FULL, ok && t2 < P);
+        const unsigned v = __ballot_sync(FULL, ok);
+        if (f) return __shfl_sync(FULL, key, __ffs(f) - 1);
+        if (v) last = __shfl_sync(FULL, key, 31 - __clz(v));
+        carry = __shfl_sync(FULL, P, 31);
     }
-    return last;
+    return last >= 0 ? last : fallback;
 }
 
-__global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
+__global__ void __launch_bounds__(256, 4) k_sample(SampleArgs a) {
     extern __shared__ float smf[];
-    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* r = smf;
     float* col = smf + (size_t)a.K * (1 + wid);
-    float* qlp = smf + (size_t)a.K * (1 + warps) + 64 * wid;  // [0,32): QL, [32,64): QP
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     __syncthreads();
     uint32_t c_tok = 0, c_ea = 0, c_full = 0, c_nnz = 0, c_max = 0, c_s = 0, c_q = 0, c_wnnz = 0;
-    uint32_t c_tdense = 0, c_tsparse = 0;
+    uint32_t c_tdense = 0, c_tsparse = 0, c_rows = 0, c_rent = 0;
     for (;;) {
         int tile = 0;
         if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
@@ -425,83 +409,118 @@ __global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
         const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
         const float QP = warp_ks_scan(QL, lane);
         const float Q = __shfl_sync(FULL, QP, 31);
-        qlp[lane] = QL;
-        qlp[32 + lane] = QP;
         if (lane == 0) col[maxK] = 0.0f;
         __syncwarp();
         double ll = 0.0;
+        uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
+        const uint32_t* row = a.dt_ent;
+        float SL = 0.0f, SP = 0.0f, S = 0.0f;
         for (uint32_t g = 0; g < cnt; g += 32) {
-            if (g + lane >= cnt) continue;
+            const bool valid = g + lane < cnt;
             const uint32_t tok = start + g + lane;
-            const uint32_t d = __ldg(a.tok_doc + tok);
-            const uint32_t m = __ldg(a.meta + tok);
-            const uint32_t nd = __ldg(a.doc_len + d);
-            const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
-            const float u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
-            const float pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
-            const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
-            const float bound = fadd(fadd(pmax, shat), Q);
-            const bool ea = fmul(u, bound) < pmax;
-            c_tok++;
-            c_ea += ea;
+            uint32_t d = 0, nd = 0;
+            float u = 0.0f, pmax = 0.0f;
+            bool ea = false;
+            if (valid) {
+                d = __ldg(a.tok_doc + tok);
+                const uint32_t m = __ldg(a.meta + tok);
+                nd = __ldg(a.doc_len + d);
+                const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
+                u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
+                pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
+                const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
+                const float bound = fadd(fadd(pmax, shat), Q);
+                ea = fmul(u, bound) < pmax;
+                c_tok++;
+                c_ea += ea;
+                if (ea && !a.ll_mode) c_max++;
+            }
             int znew = maxK;
-            if (!ea || a.ll_mode) {
-                const uint32_t nnz = __ldg(a.dt_nnz + d);
-                const uint32_t* row = a.dt_ent + __ldg(a.dt_off + d);
-                const float S = row_mass(row, nnz, col);
-                const float pS = fadd(pmax, S);
+            unsigned need = __ballot_sync(FULL, valid && (!ea || a.ll_mode));
+            while (need) {
+                const int j = __ffs(need) - 1;
+                need &= need - 1u;
+                const uint32_t dj = __shfl_sync(FULL, d, j);
+                const uint32_t ndj = __shfl_sync(FULL, nd, j);
+                const float pmj = __shfl_sync(FULL, pmax, j);
+                const float uj = __shfl_sync(FULL, u, j);
+                const bool eaj = __shfl_sync(FULL, (int)ea, j) != 0;
+                if (dj != cur) {
+                    cur = dj;
+                    nnz = __ldg(a.dt_nnz + dj);
+                    row = a.dt_ent + __ldg(a.dt_off + dj);
+                    B = (nnz + 31u) >> 5;
+                    const uint32_t b0 = lane * B, b1 = min(b0 + B, nnz);
+                    SL = 0.0f;
+                    for (uint32_t q = b0; q < b1; ++q) {
+                        const uint32_t e = __ldg(row + q);
+                        SL = ffma(u2f(e & 0xffffu), col[e >> 16], SL);
+                    }
+                    SP = warp_ks_scan(SL, lane);
+                    S = __shfl_sync(FULL, SP, 31);
+                    if (lane == 0) {
+                        c_rows++;
+                        c_rent += nnz;
+                    }
+                }
+                const float pS = fadd(pmj, S);
                 const float total = fadd(pS, Q);
-                c_full++;
-                c_nnz += nnz;
-                if (a.ll_mode) ll += log((double)total / ((double)nd + a.den_add));
-                if (!ea) {
-                    const float target = fmul(u, total);
-                    if (target < pmax) {
-                        c_max++;
+                if (lane == 0) {
+                    c_full++;
+                    c_nnz += nnz;
+                }
+                if (a.ll_mode && lane == j) ll += log((double)total / ((double)ndj + a.den_add));
+                if (!eaj) {
+                    const float target = fmul(uj, total);
+                    int zj;
+                    if (target < pmj) {
+                        zj = maxK;
+                        c_max += (lane == 0);
                     } else if (target < pS) {
-                        const int k = row_search(row, nnz, col, fsub(target, pmax));
-                        znew = k >= 0 ? k : maxK;
-                        c_s++;
+                        const float tt = fsub(target, pmj);
+                        const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
+                        const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
+                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                        const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
+                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                        const uint32_t b0 = (uint32_t)ls * B;
+                        const uint32_t nn = nnz, BB = B;
+                        const uint32_t* rr = row;
+                        zj = warp_level2(BB, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                            if (b0 + i < nn) {
+                                const uint32_t e = __ldg(rr + b0 + i);
+                                const float cz = col[e >> 16];
+                                key = (int)(e >> 16);
+                                term = fmul(u2f(e & 0xffffu), cz);
+                                ok = cz > 0.0f;
+                            }
+                        });
+                        c_s += (lane == 0);
                     } else {
                         const float tt = fsub(target, pS);
-                        int ls = -1, lastpos = -1;
-                        for (int l = 0; l < 32; ++l) {
-                            const float ql = qlp[l];
-                            if (ql > 0.0f) {
-                                lastpos = l;
-                                if (tt < qlp[32 + l]) {
-                                    ls = l;
-                                    break;
-                                }
-                            }
-                        }
-                        if (ls < 0) ls = lastpos;
-                        int found = -1, last = -1;
-                        if (ls >= 0) {
-                            const float t2 = ls > 0 ? fsub(tt, qlp[32 + ls - 1]) : tt;
-                            float acc = 0.0f;
-                            for (int k = ls; k < a.K; k += 32) {
-                                const float cz = col[k];
-                                acc = ffma(a.alpha, cz, acc);
-                                if (cz > 0.0f) {
-                                    last = k;
-                                    if (t2 < acc) {
-                                        found = k;
-                                        break;
-                                    }
-                                }
-                            }
-                        }
-                        znew = found >= 0 ? found : (last >= 0 ? last : maxK);
-                        c_q++;
+                        const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
+                        const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
+                        const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
+                        const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
+                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                        const int K = a.K;
+                        const float alpha = a.alpha;
+                        const uint32_t n = (uint32_t)((K - ls + 31) / 32);
+                        zj = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                            const int k = ls + 32 * (int)i;
+                            const float cz = col[k];
+                            key = k;
+                            term = fmul(alpha, cz);
+                            ok = cz > 0.0f;
+                        });
+                        c_q += (lane == 0);
                     }
+                    if (lane == j) znew = zj;
                 } else {
-                    c_max++;
+                    c_max += (lane == 0);
                 }
-            } else {
-                c_max++;
             }
-            a.z[tok] = (uint16_t)znew;
+            if (valid) a.z[tok] = (uint16_t)znew;
         }
         if (a.ll_mode) {
 #pragma unroll
@@ -509,9 +528,9 @@ __global__ void __launch_bounds__(256) k_sample(SampleArgs a) {
             if (lane == 0) a.tile_ll[tile] = ll;
         }
     }
-    const uint32_t vals[10] = {c_tok, c_ea, c_full, c_nnz, c_max, c_s, c_q, c_wnnz, c_tdense, c_tsparse};
+    const uint32_t vals[12] = {c_tok, c_ea, c_full, c_nnz, c_max, c_s, c_q, c_wnnz, c_tdense, c_tsparse, c_rows, c_rent};
 #pragma unroll
-    for (int i = 0; i < 10; ++i) {
+    for (int i = 0; i < 12; ++i) {
         const uint32_t s = __reduce_add_sync(FULL, vals[i]);
         if (lane == 0 && s) atomicAdd(a.ctr + i, (unsigned long long)s);
     }

@@ -22,7 +22,7 @@ using namespace lda;
 
 namespace {
 
-constexpr int kSampleTile = 4096;  // tokens per sampler tile (a word's column is rebuilt per tile)
+constexpr int kSampleTile = 512;   // tokens per sampler tile (a word's column is rebuilt per tile)
 constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
 constexpr int kCounters = 16;
 
@@ -192,7 +192,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     T.warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
     T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
-    T.smem_sample = (size_t)(T.warps + 1) * row + (size_t)T.warps * 64 * sizeof(float);
+    T.smem_sample = (size_t)(T.warps + 1) * row;
     T.smem_dt = (size_t)T.warps * row;
 
     // ---- host-side derived layout
@@ -562,6 +562,7 @@ extern "C" int lda_trainer_counters(lda_trainer* t, lda_sweep_counters* o) {
     o->tokens = (int64_t)h[0]; o->early_accept = (int64_t)h[1]; o->full = (int64_t)h[2]; o->sum_nnz_full = (int64_t)h[3];
     o->branch_max = (int64_t)h[4]; o->branch_s = (int64_t)h[5]; o->branch_q = (int64_t)h[6]; o->sum_word_nnz = (int64_t)h[7];
     o->word_tiles_dense = (int64_t)h[8]; o->word_tiles_sparse = (int64_t)h[9];
+    o->rows_evaluated = (int64_t)h[10]; o->row_entries_read = (int64_t)h[11];
     return LDA_OK;
 }
 
@@ -791,7 +792,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     const int64_t row = (int64_t)io->K * 4;
     const int warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
-    const size_t smem = (size_t)(warps + 1) * row + (size_t)warps * 64 * sizeof(float);
+    const size_t smem = (size_t)(warps + 1) * row;
     CUDA_TRY(cudaFuncSetAttribute((const void*)dev::k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = 0;
     if ((rc = occupancy_grid((const void*)dev::k_sample, 32 * warps, smem, num_sms, &grid))) return rc;

@@ -35,18 +35,20 @@
  *   shat    = fmaf((float)c2, phi_2nd, (float)rest * phi_3rd)
  *   bound   = (pmax + shat) + Q;   early accept  <=>  u*bound < pmax
  *   colz    = phi with colz[maxK] = 0
- *   S       = serial fmaf((float)cnt_e, colz[k_e], acc) over the doc row in
- *             ascending k (e = 0..nnz-1)
+ *   B       = ceil(nnz / 32); SL[l] = serial fmaf((float)cnt_e, colz[k_e], acc)
+ *             over the row entries e in [l*B, min(l*B+B, nnz)) (row ascending in k)
+ *   SP      = Kogge-Stone scan of SL; S = SP[31]
  *   pS      = pmax + S; total = pS + Q; target = u*total
  *   target < pmax -> maxK;
- *   target < pS   -> S bucket: t = target - pmax; the first row entry with
- *                    colz > 0 whose running sum (same serial fmaf) exceeds t,
- *                    else the last row entry with colz > 0;
- *   otherwise     -> Q bucket: t = target - pS; the first lane l with t < QP[l]
- *                    and QL[l] > 0 (else the last lane with QL[l] > 0), then
- *                    t2 = t - QP[l-1] and the first k = l, l+32, ... with
- *                    colz > 0 whose serial fmaf(alpha, colz[k], acc) exceeds t2
- *                    (else the last such k).
+ *   target < pS   -> S bucket, t = target - pmax, lanes (SL, SP), slots of lane l:
+ *                    the B entries of its block, term = (float)cnt * colz[k];
+ *   otherwise     -> Q bucket, t = target - pS, lanes (QL, QP), slots of lane l:
+ *                    k = l, l+32, ... < K, term = alpha * colz[k].
+ *   Bucket search: the first lane l with t < P[l] and L[l] > 0 (else the last
+ *   lane with L[l] > 0); t2 = t - P[l-1]; then rounds of 32 slots: prefix =
+ *   carry + Kogge-Stone scan of the round's terms (empty slots 0), carry = the
+ *   round's last prefix; the first slot with colz > 0 and t2 < prefix, else the
+ *   last slot with colz > 0.
  *   LL_i    = log((double)total / ((double)n_d + (double)K * (double)alpha))
  * Randoms: u = (float)(x0 >> 8) * 2^-24 with x = Philox4x32-10(ctr = {tok_lo,
  * tok_hi, iter, 0x4C444131}, key = {seed_lo, seed_hi}); initial topic =
@@ -470,6 +472,9 @@ typedef struct {
     float** fcol;
     double* wll;            /* per-word LL partial */
     orc_sample_stats* part; /* per-thread counters */
+    int32_t** key;          /* per-thread level-2 slots (K) */
+    float** term;
+    int** ok;
 } sp_ctx;
 
 /* Bucket search shared by S and Q (EZLDA/utility.cu:1456-1552): first lane
@@ -478,6 +483,27 @@ static int pick_lane(float t, const float* P, const float* L) {
     for (int l = 0; l < LANES; ++l) if (t < P[l] && L[l] > 0.0f) return l;
     for (int l = LANES - 1; l >= 0; --l) if (L[l] > 0.0f) return l;
     return -1;
+}
+
+/* Second-level bucket search in rounds of 32 slots: each round's terms are
+ * Kogge-Stone scanned and offset by the carried total of the previous rounds; the
+ * first slot that may be drawn (ok) with t2 < prefix wins, else the last ok slot. */
+static int32_t level2(int32_t n, const float* term, const int* ok, const int32_t* key, float t2,
+                      int32_t fallback) {
+    float carry = 0.0f;
+    int32_t last = -1;
+    for (int32_t base = 0; base < n; base += LANES) {
+        float tr[LANES], P[LANES];
+        for (int i = 0; i < LANES; ++i) tr[i] = base + i < n ? term[base + i] : 0.0f;
+        ks_scan32(tr, P);
+        for (int i = 0; i < LANES; ++i) P[i] = carry + P[i];
+        for (int i = 0; i < LANES && base + i < n; ++i)
+            if (ok[base + i] && t2 < P[i]) return key[base + i];
+        for (int i = 0; i < LANES && base + i < n; ++i)
+            if (ok[base + i]) last = key[base + i];
+        carry = P[LANES - 1];
+    }
+    return last >= 0 ? last : fallback;
 }
 
 static void sp_words(void* c, int64_t b, int64_t e, int tid) {
@@ -518,10 +544,19 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
             st->tokens++;
             if (ea) st->early_accept++;
             if (ea && !x->ll_mode) { x->z_out[t] = (uint16_t)maxK; st->branch_max++; continue; }
-            /* S: serial sum over the doc row in ascending k (EZLDA/utility.cu:1376-1440
-             * sums the same row in 32-entry blocks) */
-            float S = 0.0f;
-            for (int32_t q = 0; q < nnz; ++q) S = fmaf((float)(row[q] & 0xffffu), colz[row[q] >> 16], S);
+            /* S: lane l sums the contiguous block [l*B, l*B+B) of the doc row (ascending k),
+             * B = ceil(nnz/32); the lane sums are Kogge-Stone scanned (EZLDA sums the same
+             * row in 32-entry blocks, EZLDA/utility.cu:1376-1440) */
+            const int32_t B = (nnz + LANES - 1) / LANES;
+            float SL[LANES], SP[LANES];
+            for (int l = 0; l < LANES; ++l) {
+                float acc = 0.0f;
+                for (int32_t q = l * B; q < l * B + B && q < nnz; ++q)
+                    acc = fmaf((float)(row[q] & 0xffffu), colz[row[q] >> 16], acc);
+                SL[l] = acc;
+            }
+            ks_scan32(SL, SP);
+            const float S = SP[LANES - 1];
             const float pS = pmax + S;
             const float total = pS + Q;
             st->full++;
@@ -534,36 +569,45 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
                 znew = maxK;
                 st->branch_max++;
             } else if (target < pS) {
-                /* first row entry with colz > 0 whose running sum exceeds t */
                 const float tt = target - pmax;
-                float acc = 0.0f;
-                int32_t found = -1, last = -1;
-                for (int32_t q = 0; q < nnz; ++q) {
-                    const int32_t k = (int32_t)(row[q] >> 16);
-                    acc = fmaf((float)(row[q] & 0xffffu), colz[k], acc);
-                    if (colz[k] > 0.0f) {
-                        last = k;
-                        if (tt < acc) { found = k; break; }
+                const int l = pick_lane(tt, SP, SL);
+                const float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
+                znew = maxK;
+                if (l >= 0) {
+                    int32_t* key = x->key[tid];
+                    float* term = x->term[tid];
+                    int* ok = x->ok[tid];
+                    for (int32_t i = 0; i < B; ++i) {
+                        const int32_t q = l * B + i;
+                        key[i] = -1; term[i] = 0.0f; ok[i] = 0;
+                        if (q < nnz) {
+                            const int32_t k = (int32_t)(row[q] >> 16);
+                            key[i] = k;
+                            term[i] = (float)(row[q] & 0xffffu) * colz[k];
+                            ok[i] = colz[k] > 0.0f;
+                        }
                     }
+                    znew = level2(B, term, ok, key, t2, maxK);
                 }
-                znew = found >= 0 ? found : last;
-                if (znew < 0) znew = maxK; /* no positive bin (cannot happen for beta > 0) */
                 st->branch_s++;
             } else {
                 const float tt = target - pS;
-                int l = pick_lane(tt, QP, QL);
-                float t2 = tt - (l > 0 ? QP[l - 1] : 0.0f);
-                float acc = 0.0f;
-                int32_t found = -1, last = -1;
-                for (int32_t k = l; l >= 0 && k < K; k += LANES) {
-                    acc = fmaf(alpha, colz[k], acc);
-                    if (colz[k] > 0.0f) {
-                        last = k;
-                        if (t2 < acc) { found = k; break; }
+                const int l = pick_lane(tt, QP, QL);
+                const float t2 = tt - (l > 0 ? QP[l - 1] : 0.0f);
+                znew = maxK;
+                if (l >= 0) {
+                    int32_t* key = x->key[tid];
+                    float* term = x->term[tid];
+                    int* ok = x->ok[tid];
+                    const int32_t n = (K - l + LANES - 1) / LANES;
+                    for (int32_t i = 0; i < n; ++i) {
+                        const int32_t k = l + LANES * i;
+                        key[i] = k;
+                        term[i] = alpha * colz[k];
+                        ok[i] = colz[k] > 0.0f;
                     }
+                    znew = level2(n, term, ok, key, t2, maxK);
                 }
-                znew = found >= 0 ? found : last;
-                if (znew < 0) znew = maxK;
                 st->branch_q++;
             }
             x->z_out[t] = (uint16_t)znew;
@@ -583,9 +627,15 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
     x.fcol = (float**)calloc((size_t)nt, sizeof(float*));
     x.part = (orc_sample_stats*)calloc((size_t)nt, sizeof(orc_sample_stats));
     x.wll = (double*)calloc((size_t)s->V, sizeof(double));
+    x.key = (int32_t**)calloc((size_t)nt, sizeof(int32_t*));
+    x.term = (float**)calloc((size_t)nt, sizeof(float*));
+    x.ok = (int**)calloc((size_t)nt, sizeof(int*));
     for (int t = 0; t < nt; ++t) {
         x.icnt[t] = (int32_t*)calloc((size_t)s->K, sizeof(int32_t));
         x.fcol[t] = (float*)calloc((size_t)s->K, sizeof(float));
+        x.key[t] = (int32_t*)calloc((size_t)s->K + LANES, sizeof(int32_t));
+        x.term[t] = (float*)calloc((size_t)s->K + LANES, sizeof(float));
+        x.ok[t] = (int*)calloc((size_t)s->K + LANES, sizeof(int));
     }
     parallel_for(nt, s->V, 16, sp_words, &x);
     orc_sample_stats tot;
@@ -598,10 +648,10 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
         tot.branch_max += x.part[t].branch_max;
         tot.branch_s += x.part[t].branch_s;
         tot.branch_q += x.part[t].branch_q;
-        free(x.icnt[t]); free(x.fcol[t]);
+        free(x.icnt[t]); free(x.fcol[t]); free(x.key[t]); free(x.term[t]); free(x.ok[t]);
     }
     for (int32_t w = 0; w < s->V; ++w) tot.loglik += x.wll[w];
-    free(x.icnt); free(x.fcol); free(x.part); free(x.wll);
+    free(x.icnt); free(x.fcol); free(x.part); free(x.wll); free(x.key); free(x.term); free(x.ok);
     if (st) *st = tot;
     return 0;
 }
