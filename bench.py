@@ -49,6 +49,7 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-word-stride", type=int, default=40)
     p.add_argument("--preset", default="c1")
+    p.add_argument("--chunks", type=int, default=0, help="override the preset's chunk count")
     return p.parse_args()
 
 
@@ -138,10 +139,13 @@ def physical_gpu(local: int) -> int:
     return local
 
 
-def make_corpus(preset: str, rank: int):
+def make_corpus(preset: str, rank: int, chunks: int = 0):
     import lda_sc20_b200 as L
     base = L.corpus_config(preset)
-    return L.Corpus.generate(L.corpus_config(preset, corpus_seed=base.corpus_seed + rank))
+    over = {"corpus_seed": base.corpus_seed + rank}
+    if chunks > 0:
+        over["num_chunks"] = chunks
+    return L.Corpus.generate(L.corpus_config(preset, **over))
 
 
 def sampler_algorithmic_bytes(cnt, K: int, dense_words_per_sweep: int, sweeps: int, launches: int) -> float:
@@ -164,7 +168,7 @@ def run_ours(args, world, rank, local):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
-    corpus = make_corpus(args.preset, rank)
+    corpus = make_corpus(args.preset, rank, args.chunks)
     info = corpus.info
     K = info.K_hint
     N = info.num_tokens
@@ -226,6 +230,20 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     ms_ll_sweep = e2.elapsed_time(e3) / n_ll
 
+    # per-sweep device time over a fresh run of the same sweeps (diagnostic, not the metric)
+    tr.set_topics(z0)
+    tr.iteration = 0
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
+        check_iter(tr, 1)
+        evs[i + 1].record(stream)
+    torch.cuda.synchronize()
+    per_sweep = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
+    marks = sorted({i for i in (0, 1, 2, 5, 10, 20, 50, 99, args.steps - 1) if i < args.steps})
+    trace = {str(i): round(per_sweep[i], 3) for i in marks}
+
     sweeps = args.steps
     value = world * N * sweeps / (ms / 1e3)
     launches_sample = tm.launches_sample
@@ -284,8 +302,10 @@ def run_ours(args, world, rank, local):
                          "ms_per_launch": ms_per_launch},
             "stages_ms_per_sweep": {"wt": tm.ms_wt / sweeps, "stats": tm.ms_stats / sweeps,
                                     "dt": tm.ms_dt / sweeps, "sample": tm.ms_sample / sweeps},
+            "sweep_ms_trace": trace,
             "sweep_counters": {"early_accept_frac": cnt.early_accept / max(cnt.tokens, 1),
                                "mean_nnz_full": cnt.sum_nnz_full / max(cnt.full, 1),
+                               "rows_per_evaluated_token": cnt.rows_evaluated / max(cnt.full, 1),
                                "branch_max": cnt.branch_max, "branch_s": cnt.branch_s, "branch_q": cnt.branch_q},
             "clocks": clk,
             "cpu_baseline": cpu,
@@ -295,6 +315,11 @@ def run_ours(args, world, rank, local):
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def check_iter(tr, n):
+    """n sweeps enqueued without waiting (the C ABI call returns after its own sync)."""
+    tr.iterate(n)
 
 
 def cpu_baseline(corpus, tr, z0, K, sweeps, stride):

@@ -323,11 +323,11 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
 //   S      lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
 //          one Kogge-Stone scan gives the lane prefixes; a doc row is evaluated once
 //          for consecutive tokens of the same (word, doc) in the tile;
-//   search ballot over the lane prefixes picks the block, then each lane takes one
-//          entry of it and a second scan plus a ballot pick the topic (32 entries per
-//          round, carried across rounds);
-//   Q      the same two levels over the per-word lane prefixes of Q and the lane's
-//          topics k = l, l+32, ...
+//   bucket a ballot over the lane prefixes picks the block of an S-bucket draw; the
+//          in-block draw (at most B entries) runs afterwards thread-per-token, all the
+//          group's S-bucket tokens at once;
+//   Q      a ballot over the per-word lane prefixes of Q, then one topic per lane with a
+//          scan and a ballot (topics k = l, l+32, ..., 32 per round, carried).
 // Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain
 // (EZLDA/utility.cu:2680-3312, :1625-2103, :1217-1611) in one pass, with no
 // effective-token list in global memory and no spin lock.
@@ -381,15 +381,65 @@ __device__ __forceinline__ int warp_level2(uint32_t n, float t2, int fallback, i
     return last >= 0 ? last : fallback;
 }
 
-__global__ void __launch_bounds__(256, 4) k_sample(SampleArgs a) {
+// Sweep counters live in shared memory (one row per warp, written by lane 0) so they
+// cost no registers in the sampling loop.
+enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE, C_ROWS, C_RENT, C_NUM };
+
+#ifndef LDA_SAMPLE_MIN_BLOCKS
+#define LDA_SAMPLE_MIN_BLOCKS 4
+#endif
+
+// Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
+// loads of two entries are issued together).
+__device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
+                                            const float* col) {
+    float acc = 0.0f;
+    uint32_t q = b0;
+    for (; q + 2 <= b1; q += 2) {
+        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 1);
+        acc = ffma(u2f(e0 & 0xffffu), col[e0 >> 16], acc);
+        acc = ffma(u2f(e1 & 0xffffu), col[e1 >> 16], acc);
+    }
+    if (q < b1) {
+        const uint32_t e = __ldg(row + q);
+        acc = ffma(u2f(e & 0xffffu), col[e >> 16], acc);
+    }
+    return acc;
+}
+
+// The S-bucket draw inside one lane block: the block's serial partial sums (the same
+// fmaf chain as block_mass) are compared with t2; the first entry with colz > 0 whose
+// partial sum exceeds t2 wins, else the last entry with colz > 0, else `fallback`.
+__device__ __forceinline__ int block_draw(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
+                                          const float* col, float t2, int fallback) {
+    float acc = 0.0f;
+    int last = -1;
+    for (uint32_t q = b0; q < b1; ++q) {
+        const uint32_t e = __ldg(row + q);
+        const int k = (int)(e >> 16);
+        const float cz = col[k];
+        acc = ffma(u2f(e & 0xffffu), cz, acc);
+        if (cz > 0.0f) {
+            last = k;
+            if (t2 < acc) return k;
+        }
+    }
+    return last >= 0 ? last : fallback;
+}
+
+// Branch taken by a token (counters only).
+enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
+
+template <bool LL>
+__global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleArgs a) {
     extern __shared__ float smf[];
-    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* r = smf;
     float* col = smf + (size_t)a.K * (1 + wid);
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smf + (size_t)a.K * (1 + warps)) + C_NUM * wid;
     fill_recip(r, a.n_k, a.K, a.Vbeta);
+    if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();
-    uint32_t c_tok = 0, c_ea = 0, c_full = 0, c_nnz = 0, c_max = 0, c_s = 0, c_q = 0, c_wnnz = 0;
-    uint32_t c_tdense = 0, c_tsparse = 0, c_rows = 0, c_rent = 0;
     for (;;) {
         int tile = 0;
         if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
@@ -399,10 +449,11 @@ __global__ void __launch_bounds__(256, 4) k_sample(SampleArgs a) {
         const int w = t.x;
         const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
         __syncwarp();
-        build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &c_wnnz);
+        uint32_t wnnz = 0;
+        build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
         if (lane == 0) {
-            c_tdense += (w < a.Vd);
-            c_tsparse += (w >= a.Vd);
+            ctr[C_WNNZ] += wnnz;
+            ctr[w < a.Vd ? C_TDENSE : C_TSPARSE] += 1u;
         }
         const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
         const float4 ph = __ldg(a.st_phi + w);
@@ -418,122 +469,123 @@ __global__ void __launch_bounds__(256, 4) k_sample(SampleArgs a) {
         for (uint32_t g = 0; g < cnt; g += 32) {
             const bool valid = g + lane < cnt;
             const uint32_t tok = start + g + lane;
-            uint32_t d = 0, nd = 0;
+            uint32_t d = 0xffffffffu, nd = 0, my_nnz = 0, my_off = 0;
             float u = 0.0f, pmax = 0.0f;
             bool ea = false;
             if (valid) {
                 d = __ldg(a.tok_doc + tok);
                 const uint32_t m = __ldg(a.meta + tok);
                 nd = __ldg(a.doc_len + d);
+                my_nnz = __ldg(a.dt_nnz + d);
+                my_off = __ldg(a.dt_off + d);
                 const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
                 u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
                 pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
                 const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
                 const float bound = fadd(fadd(pmax, shat), Q);
                 ea = fmul(u, bound) < pmax;
-                c_tok++;
-                c_ea += ea;
-                if (ea && !a.ll_mode) c_max++;
             }
             int znew = maxK;
-            unsigned need = __ballot_sync(FULL, valid && (!ea || a.ll_mode));
+            // per-lane record of this token's evaluation, for the deferred draw and counters
+            const uint32_t* my_row = row;
+            uint32_t my_b0 = 0, my_b1 = 0;
+            float my_t2 = 0.0f;
+            int kind = BR_NONE;
+            bool evaluated = false;
+            const unsigned vmask = __ballot_sync(FULL, valid);
+            const unsigned emask = __ballot_sync(FULL, ea);
+            const unsigned need0 = LL ? vmask : (vmask & ~emask);
+            unsigned need = need0;
             while (need) {
                 const int j = __ffs(need) - 1;
                 need &= need - 1u;
                 const uint32_t dj = __shfl_sync(FULL, d, j);
-                const uint32_t ndj = __shfl_sync(FULL, nd, j);
-                const float pmj = __shfl_sync(FULL, pmax, j);
-                const float uj = __shfl_sync(FULL, u, j);
-                const bool eaj = __shfl_sync(FULL, (int)ea, j) != 0;
                 if (dj != cur) {
                     cur = dj;
-                    nnz = __ldg(a.dt_nnz + dj);
-                    row = a.dt_ent + __ldg(a.dt_off + dj);
+                    nnz = __shfl_sync(FULL, my_nnz, j);
+                    row = a.dt_ent + __shfl_sync(FULL, my_off, j);
                     B = (nnz + 31u) >> 5;
-                    const uint32_t b0 = lane * B, b1 = min(b0 + B, nnz);
-                    SL = 0.0f;
-                    for (uint32_t q = b0; q < b1; ++q) {
-                        const uint32_t e = __ldg(row + q);
-                        SL = ffma(u2f(e & 0xffffu), col[e >> 16], SL);
-                    }
+                    const uint32_t b0 = min(lane * B, nnz);
+                    SL = block_mass(row, b0, min(b0 + B, nnz), col);
                     SP = warp_ks_scan(SL, lane);
                     S = __shfl_sync(FULL, SP, 31);
-                    if (lane == 0) {
-                        c_rows++;
-                        c_rent += nnz;
-                    }
+                    evaluated |= (lane == j);
                 }
+                const float pmj = __shfl_sync(FULL, pmax, j);
+                const float uj = __shfl_sync(FULL, u, j);
                 const float pS = fadd(pmj, S);
                 const float total = fadd(pS, Q);
-                if (lane == 0) {
-                    c_full++;
-                    c_nnz += nnz;
+                if (LL) {
+                    if (lane == j) ll += log((double)total / ((double)nd + a.den_add));
                 }
-                if (a.ll_mode && lane == j) ll += log((double)total / ((double)ndj + a.den_add));
-                if (!eaj) {
-                    const float target = fmul(uj, total);
-                    int zj;
-                    if (target < pmj) {
-                        zj = maxK;
-                        c_max += (lane == 0);
-                    } else if (target < pS) {
-                        const float tt = fsub(target, pmj);
-                        const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
-                        const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
-                        const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
-                        const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
-                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
-                        const uint32_t b0 = (uint32_t)ls * B;
-                        const uint32_t nn = nnz, BB = B;
-                        const uint32_t* rr = row;
-                        zj = warp_level2(BB, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
-                            if (b0 + i < nn) {
-                                const uint32_t e = __ldg(rr + b0 + i);
-                                const float cz = col[e >> 16];
-                                key = (int)(e >> 16);
-                                term = fmul(u2f(e & 0xffffu), cz);
-                                ok = cz > 0.0f;
-                            }
-                        });
-                        c_s += (lane == 0);
-                    } else {
-                        const float tt = fsub(target, pS);
-                        const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
-                        const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
-                        const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
-                        const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
-                        const float t2 = ls > 0 ? fsub(tt, prev) : tt;
-                        const int K = a.K;
-                        const float alpha = a.alpha;
-                        const uint32_t n = (uint32_t)((K - ls + 31) / 32);
-                        zj = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
-                            const int k = ls + 32 * (int)i;
-                            const float cz = col[k];
-                            key = k;
-                            term = fmul(alpha, cz);
-                            ok = cz > 0.0f;
-                        });
-                        c_q += (lane == 0);
+                if (LL && ((emask >> j) & 1u)) continue;
+                const float target = fmul(uj, total);
+                if (target < pmj) {
+                    if (lane == j) kind = BR_MAX;
+                } else if (target < pS) {
+                    const float tt = fsub(target, pmj);
+                    const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
+                    const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
+                    const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                    const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
+                    if (lane == j) {
+                        kind = BR_S;
+                        my_row = row;
+                        my_b0 = (uint32_t)ls * B;
+                        my_b1 = min(my_b0 + B, nnz);
+                        my_t2 = ls > 0 ? fsub(tt, prev) : tt;
                     }
-                    if (lane == j) znew = zj;
                 } else {
-                    c_max += (lane == 0);
+                    const float tt = fsub(target, pS);
+                    const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
+                    const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
+                    const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
+                    const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
+                    const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                    const int K = a.K;
+                    const float alpha = a.alpha;
+                    const uint32_t n = (uint32_t)((K - ls + 31) / 32);
+                    const int zq = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                        const int k = ls + 32 * (int)i;
+                        const float cz = col[k];
+                        key = k;
+                        term = fmul(alpha, cz);
+                        ok = cz > 0.0f;
+                    });
+                    if (lane == j) {
+                        kind = BR_Q;
+                        znew = zq;
+                    }
                 }
             }
+            if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, col, my_t2, maxK);
             if (valid) a.z[tok] = (uint16_t)znew;
+            // counters of the group: ballots and warp sums instead of per-token updates
+            const bool in_need = (need0 >> lane) & 1u;
+            const unsigned sm = __ballot_sync(FULL, kind == BR_S), qm = __ballot_sync(FULL, kind == BR_Q);
+            const unsigned xm = __ballot_sync(FULL, kind == BR_MAX), rm = __ballot_sync(FULL, evaluated);
+            const uint32_t nnz_full = __reduce_add_sync(FULL, in_need ? my_nnz : 0u);
+            const uint32_t nnz_rows = __reduce_add_sync(FULL, evaluated ? my_nnz : 0u);
+            if (lane == 0) {
+                ctr[C_TOK] += __popc(vmask);
+                ctr[C_EA] += __popc(emask);
+                ctr[C_FULL] += __popc(need0);
+                ctr[C_NNZ] += nnz_full;
+                ctr[C_MAX] += __popc(xm) + __popc(emask);
+                ctr[C_S] += __popc(sm);
+                ctr[C_Q] += __popc(qm);
+                ctr[C_ROWS] += __popc(rm);
+                ctr[C_RENT] += nnz_rows;
+            }
         }
-        if (a.ll_mode) {
+        if (LL) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);
             if (lane == 0) a.tile_ll[tile] = ll;
         }
     }
-    const uint32_t vals[12] = {c_tok, c_ea, c_full, c_nnz, c_max, c_s, c_q, c_wnnz, c_tdense, c_tsparse, c_rows, c_rent};
-#pragma unroll
-    for (int i = 0; i < 12; ++i) {
-        const uint32_t s = __reduce_add_sync(FULL, vals[i]);
-        if (lane == 0 && s) atomicAdd(a.ctr + i, (unsigned long long)s);
-    }
+    __syncwarp();
+    if (lane < C_NUM && ctr[lane]) atomicAdd(a.ctr + lane, (unsigned long long)ctr[lane]);
 }
 
 // Fixed-order FP64 reduction of the per-tile LL partials (one CTA of 1024 threads).

@@ -192,7 +192,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     T.warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
     T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
-    T.smem_sample = (size_t)(T.warps + 1) * row;
+    T.smem_sample = (size_t)(T.warps + 1) * row + (size_t)T.warps * 16 * sizeof(uint32_t);
     T.smem_dt = (size_t)T.warps * row;
 
     // ---- host-side derived layout
@@ -295,12 +295,16 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     // ---- launch shapes: persistent grids sized by occupancy
     const int threads = 32 * T.warps;
     for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
-                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair((const void*)dev::k_sample, T.smem_sample)})
+                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair((const void*)dev::k_sample_t<false>, T.smem_sample),
+                    std::make_pair((const void*)dev::k_sample_t<true>, T.smem_sample)})
         CUDA_TRY(cudaFuncSetAttribute(kv.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kv.second));
     if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
-    if ((rc = occupancy_grid((const void*)dev::k_sample, threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+    if ((rc = occupancy_grid((const void*)dev::k_sample_t<false>, threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+    int grid_ll = 0;
+    if ((rc = occupancy_grid((const void*)dev::k_sample_t<true>, threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
+    T.grid_sample = std::min(T.grid_sample, grid_ll);
     T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
     CUDA_TRY(cudaDeviceSynchronize());
     T.chunk_sampled_ll.assign(T.C, false);
@@ -405,7 +409,8 @@ extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) 
     a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = t->dt_ent; a.ctr = t->ctr;
     if (n > 0) {
         const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
-        dev::k_sample<<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
+        if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
+        else dev::k_sample_t<false><<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
         CUDA_TRY(cudaGetLastError());
     }
     t->end_stage();
@@ -792,10 +797,11 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     const int64_t row = (int64_t)io->K * 4;
     const int warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
-    const size_t smem = (size_t)(warps + 1) * row;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)dev::k_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t smem = (size_t)(warps + 1) * row + (size_t)warps * 16 * sizeof(uint32_t);
+    const void* kfn = io->ll_mode ? (const void*)dev::k_sample_t<true> : (const void*)dev::k_sample_t<false>;
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int grid = 0;
-    if ((rc = occupancy_grid((const void*)dev::k_sample, 32 * warps, smem, num_sms, &grid))) return rc;
+    if ((rc = occupancy_grid(kfn, 32 * warps, smem, num_sms, &grid))) return rc;
     grid = std::max(1, std::min(grid, (io->num_tiles + warps - 1) / warps));
     dev::SampleArgs a;
     a.tiles = reinterpret_cast<const int4*>(io->tiles);
@@ -812,7 +818,8 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.tok_doc = io->tok_doc; a.meta = io->meta; a.z = io->topics; a.doc_len = io->doc_len;
     a.dt_off = io->dt_off; a.dt_nnz = io->dt_nnz; a.dt_ent = io->dt_ent;
     a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
-    dev::k_sample<<<grid, 32 * warps, smem, st>>>(a);
+    if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * warps, smem, st>>>(a);
+    else dev::k_sample_t<false><<<grid, 32 * warps, smem, st>>>(a);
     CUDA_TRY(cudaGetLastError());
     if (io->ll_mode) {
         dev::k_ll_reduce<<<1, 1024, 0, st>>>(a.tile_ll, io->num_tiles, io->ll_sum);

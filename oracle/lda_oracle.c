@@ -40,15 +40,16 @@
  *   SP      = Kogge-Stone scan of SL; S = SP[31]
  *   pS      = pmax + S; total = pS + Q; target = u*total
  *   target < pmax -> maxK;
- *   target < pS   -> S bucket, t = target - pmax, lanes (SL, SP), slots of lane l:
- *                    the B entries of its block, term = (float)cnt * colz[k];
+ *   target < pS   -> S bucket, t = target - pmax, lanes (SL, SP); in block l the
+ *                    serial partial sums of SL[l]'s fmaf chain are compared with t2;
  *   otherwise     -> Q bucket, t = target - pS, lanes (QL, QP), slots of lane l:
- *                    k = l, l+32, ... < K, term = alpha * colz[k].
- *   Bucket search: the first lane l with t < P[l] and L[l] > 0 (else the last
- *   lane with L[l] > 0); t2 = t - P[l-1]; then rounds of 32 slots: prefix =
- *   carry + Kogge-Stone scan of the round's terms (empty slots 0), carry = the
- *   round's last prefix; the first slot with colz > 0 and t2 < prefix, else the
- *   last slot with colz > 0.
+ *                    k = l, l+32, ... < K, term = alpha * colz[k], in rounds of 32
+ *                    slots: prefix = carry + Kogge-Stone scan of the round's terms
+ *                    (empty slots 0), carry = the round's last prefix.
+ *   Lane choice: the first lane l with t < P[l] and L[l] > 0 (else the last lane
+ *   with L[l] > 0); t2 = t - P[l-1].  In the lane: the first entry/slot with
+ *   colz > 0 whose partial sum / prefix exceeds t2, else the last one with
+ *   colz > 0, else maxK.
  *   LL_i    = log((double)total / ((double)n_d + (double)K * (double)alpha))
  * Randoms: u = (float)(x0 >> 8) * 2^-24 with x = Philox4x32-10(ctr = {tok_lo,
  * tok_hi, iter, 0x4C444131}, key = {seed_lo, seed_hi}); initial topic =
@@ -574,20 +575,18 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
                 const float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
                 znew = maxK;
                 if (l >= 0) {
-                    int32_t* key = x->key[tid];
-                    float* term = x->term[tid];
-                    int* ok = x->ok[tid];
-                    for (int32_t i = 0; i < B; ++i) {
-                        const int32_t q = l * B + i;
-                        key[i] = -1; term[i] = 0.0f; ok[i] = 0;
-                        if (q < nnz) {
-                            const int32_t k = (int32_t)(row[q] >> 16);
-                            key[i] = k;
-                            term[i] = (float)(row[q] & 0xffffu) * colz[k];
-                            ok[i] = colz[k] > 0.0f;
+                    /* the block's serial partial sums (the fmaf chain of SL[l]) */
+                    float acc = 0.0f;
+                    int32_t found = -1, last = -1;
+                    for (int32_t q = l * B; q < l * B + B && q < nnz; ++q) {
+                        const int32_t k = (int32_t)(row[q] >> 16);
+                        acc = fmaf((float)(row[q] & 0xffffu), colz[k], acc);
+                        if (colz[k] > 0.0f) {
+                            last = k;
+                            if (t2 < acc) { found = k; break; }
                         }
                     }
-                    znew = level2(B, term, ok, key, t2, maxK);
+                    znew = found >= 0 ? found : (last >= 0 ? last : maxK);
                 }
                 st->branch_s++;
             } else {
