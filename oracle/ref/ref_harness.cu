@@ -25,6 +25,9 @@
 //   dist   <chunkdir> <outdir> <reps> <stride>
 //                                         reps independent sweeps from the initial topics;
 //                                         histogram of the new topic of every stride-th token
+//   time   <chunkdir> <outdir> <n>        n sweeps on EZLDA's two-stream schedule, timed
+//                                         with its iterStart/iterStop events
+//                                         (EZLDA/mainKernel.cu:158-347); writes per-sweep ms
 #include "DTUpdateKernel.cuh"
 #include "WTUpdateKernel.cuh"
 #include "WTDenUpdateKernel.cuh"
@@ -226,6 +229,67 @@ struct Ref {
     }
 };
 
+// EZLDA/mainKernel.cu:158-347 with its two streams and events: prologue on stream 1,
+// chunk c on stream c % 2 (the first chunk of stream 0 waits for the prologue), stream 1
+// waits for stream 0's last chunk, iteration time between iterStart and iterStop.
+static void mode_time(Ref& r, const string& out, int n) {
+    if (r.s.numD != 0) { fprintf(stderr, "time mode needs a corpus without dense words\n"); exit(2); }
+    cudaStream_t streams[numStreams];
+    for (int i = 0; i < numStreams; i++) CK(cudaStreamCreateWithPriority(&streams[i], cudaStreamDefault, i));
+    cudaEvent_t startEvent, iterStart, iterStop, stopEvents[numStreams];
+    CK(cudaEventCreate(&startEvent));
+    CK(cudaEventCreate(&iterStart));
+    CK(cudaEventCreate(&iterStop));
+    for (int i = 0; i < numStreams; i++) CK(cudaEventCreate(&stopEvents[i]));
+    r.initial_wt();
+    vector<float> ms(n);
+    for (int it = 0; it < n; it++) {
+        CK(cudaEventRecord(iterStart, streams[1]));
+        r.wt->GPUMemset(streams[1]);
+        if (it > 0)
+            for (int sid = 0; sid < numStreams; sid++) initRandState<<<GridDim + 3, BlockDim, 0, streams[sid]>>>(r.rs[sid]);
+        UpdateWTDenRowSumKernel(*r.wtd, *r.wt, streams[1]);
+        for (int c = 0; c < r.s.numChunks; c++) {
+            const int sid = c % numStreams;
+            r.wt->chunkCPU2GPUCountOffset(c, sid, streams[1]);
+            r.wt->chunkGPUMemset(sid, streams[1]);
+            r.wt->chunkWTCPU2GPU(c, sid, streams[1]);
+            WTAdditionKernel(*r.wt, *r.doc, sid, streams[1]);
+        }
+        r.doc->CPU2GPUPerplexity(streams[1]);
+        CK(cudaEventRecord(startEvent, streams[1]));
+        for (int c = 0; c < r.s.numChunks; c++) {
+            const int sid = c % numStreams;
+            cudaStream_t& st = streams[sid];
+            r.doc->CPU2GPU(c, sid, st);
+            r.dt->GPUMemSet(c, sid, st);
+            r.dt->CPU2GPUDTCountOffset(c, sid, st);
+            if (c < numStreams && sid != 1) CK(cudaStreamWaitEvent(st, startEvent, 0));
+            MaxTopicKernel(*r.wt, *r.doc, *r.wtd, sid, st);
+            UpdateDTKernel(*r.dt, *r.doc, sid, st);
+            SampleKernel(*r.wt, *r.dt, *r.doc, r.rs[sid], sid, st);
+            r.wt->chunkCPU2GPUCountOffset(c, sid, st);
+            r.wt->chunkGPUMemset(sid, st);
+            UpdateWTKernel(*r.wt, *r.doc, c, sid, st);
+            r.wt->chunkWTGPU2CPU(c, sid, st);
+            if (sid != 1) CK(cudaEventRecord(stopEvents[sid], st));
+            r.doc->GPU2CPU(c, sid, st);
+        }
+        for (int sid = 0; sid < numStreams; sid++)
+            if (sid != 1) CK(cudaStreamWaitEvent(streams[1], stopEvents[sid], 0));
+        CK(cudaEventRecord(iterStop, streams[1]));
+        CK(cudaEventSynchronize(iterStop));
+        CK(cudaEventElapsedTime(&ms[it], iterStart, iterStop));
+        r.wtd->GPUMemCopy(streams[1]);
+        r.wtd->GPUMemset(streams[1]);
+        CK(cudaStreamSynchronize(streams[1]));
+    }
+    dump_host(out + "/sweep_ms.f32", ms.data(), ms.size());
+    vector<unsigned short> z = r.topics();
+    dump_host(out + "/topics_last.u16", z.data(), z.size());
+    printf("time ok: %d sweeps of %zu tokens\n", n, r.tokens());
+}
+
 static void mode_counts(Ref& r, const string& out) {
     r.initial_wt();
     r.prologue();
@@ -300,6 +364,7 @@ int main(int argc, char** argv) {
     if (mode == "counts") mode_counts(r, out);
     else if (mode == "sweeps" && argc >= 5) mode_sweeps(r, out, atoi(argv[4]));
     else if (mode == "dist" && argc >= 6) mode_dist(r, out, atoi(argv[4]), atoi(argv[5]));
+    else if (mode == "time" && argc >= 5) mode_time(r, out, atoi(argv[4]));
     else { fprintf(stderr, "bad mode\n"); return 2; }
     CK(cudaDeviceSynchronize());
     return 0;

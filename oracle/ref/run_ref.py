@@ -42,6 +42,10 @@ BETA = np.float32(0.01)
 REF_COUNTS = dict(preset="c1", num_docs=200, vocab=3000, num_chunks=2, dense_kind=0, corpus_seed=2024)
 REF_SWEEPS = dict(preset="c1", num_docs=8000, vocab=20000, phi_kind=0, phi_conc=0.05, num_chunks=8,
                   dense_kind=2, dense_param=0.0, corpus_seed=3030)
+# EZLDA's timing on the same B200: the largest corpus shape its sparse path handles
+# (every word under K occurrences per chunk, no dense words), K=1024, 8 chunks, ~14.5M tokens
+REF_TIME = dict(preset="c1", num_docs=60000, vocab=100000, phi_kind=0, phi_conc=0.05, num_chunks=8,
+                dense_kind=2, dense_param=0.0, corpus_seed=5050)
 REF_DIST = dict(preset="c0", num_docs=50, vocab=300, K=K, len_p1=50.0, num_chunks=2, dense_kind=2,
                 dense_param=0.0, corpus_seed=4040)
 
@@ -232,6 +236,57 @@ def mode_dist(tmp, out, reps=2000, stride=25):
             "frac_p_below_0.01": float((pvals < 0.01).mean())}
 
 
+def mode_time(tmp, out, n=30):
+    """EZLDA's per-sweep time (its own iterStart/iterStop events over its two-stream
+    schedule, host<->device chunk copies included) against this library on the same
+    corpus and sweeps: resident (lda_trainer_iterate) and through host buffers
+    (lda_iterate_host, topics uploaded and downloaded every sweep)."""
+    import time as _time
+    import torch
+    c = make_corpus(REF_TIME)
+    i = c.info
+    d = os.path.join(tmp, "time")
+    c.write_ezlda(d, K)
+    dump = os.path.join(tmp, "time_out")
+    os.makedirs(dump)
+    log = run_harness("time", d, dump, n)
+    ref_ms = np.fromfile(os.path.join(dump, "sweep_ms.f32"), dtype=np.float32)
+    z_ref = np.fromfile(os.path.join(dump, "topics_last.u16"), dtype=np.uint16) - 1
+    tr = L.Trainer(c, K=K, alpha=float(ALPHA), beta=float(BETA), seed=42)
+    stream = torch.cuda.current_stream()
+    tr.set_stream(stream.cuda_stream)
+    z0 = c.topics()
+    tr.iterate(2)
+    tr.set_topics(z0)
+    tr.iteration = 0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    tr.iterate(n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ours_ms = e0.elapsed_time(e1) / n
+    z_ours = tr.topics()
+    a = torch.from_numpy(z0.view(np.int16).copy()).pin_memory()
+    b = torch.empty_like(a).pin_memory()
+    tr.iteration = 0
+    t0 = _time.perf_counter()
+    for _ in range(n):
+        tr.iterate_host(a.numpy().view(np.uint16), b.numpy().view(np.uint16))
+        a, b = b, a
+    e2e_ms = 1e3 * (_time.perf_counter() - t0) / n
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, ALPHA, BETA)
+    ll_ref, ll_ours = oracle_ll(o, z_ref.astype(np.uint16)), oracle_ll(o, z_ours)
+    res = {"log": log.strip(), "tokens": i.num_tokens, "sweeps": n,
+           "ref_ms_per_sweep": float(ref_ms.mean()), "ref_ms_first_last": [float(ref_ms[0]), float(ref_ms[-1])],
+           "ours_ms_per_sweep": ours_ms, "ours_e2e_ms_per_sweep": e2e_ms,
+           "speedup_resident": float(ref_ms.mean()) / ours_ms, "speedup_e2e": float(ref_ms.mean()) / e2e_ms,
+           "ll_after": {"ref": ll_ref, "ours": ll_ours}}
+    with open(os.path.join(out, "ref_time.json"), "w") as f:
+        json.dump({"params": REF_TIME, **res}, f, indent=1)
+    return res
+
+
 def _chi2_pvalue(h, p, n, chi2):
     """Pearson chi-square with bins of expected count < 5 pooled into one."""
     exp = p * n
@@ -256,7 +311,7 @@ def main():
     summary = {}
     try:
         for m in modes.split(","):
-            fn = {"counts": mode_counts, "sweeps": mode_sweeps, "dist": mode_dist}[m]
+            fn = {"counts": mode_counts, "sweeps": mode_sweeps, "dist": mode_dist, "time": mode_time}[m]
             try:
                 summary[m] = fn(tmp, out)
             except Exception as e:  # record and continue with the other modes
