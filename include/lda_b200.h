@@ -121,7 +121,7 @@ typedef struct {
     int64_t device_budget;  /* bytes the trainer may allocate (0: no limit) */
 } lda_train_config;
 
-/* Per-sweep counters of the last lda_trainer_iterate / lda_sample_chunk calls. */
+/* Sweep counters accumulated since the trainer was created or lda_trainer_reset_stats. */
 typedef struct {
     int64_t tokens;        /* tokens sampled */
     int64_t early_accept;  /* settled by the max-topic bound */
@@ -156,6 +156,15 @@ int lda_trainer_set_stream(lda_trainer* t, void* cuda_stream);
 int lda_trainer_get_stream(lda_trainer* t, void** cuda_stream);
 /* Bytes of device memory held by the trainer. */
 int lda_trainer_device_bytes(const lda_trainer* t, int64_t* bytes);
+/* Restricts lda_trainer_iterate's doc-topic rebuild, sampling and log-likelihood to
+ * chunks [first, last) (default: all).  The word-topic rebuild always reads every
+ * chunk's topics.  A document-sharded run gives each rank a disjoint range and
+ * exchanges the ranges' topics after every sweep (EZLDA is single-GPU; this is the
+ * exchange step of its multi-GPU form). */
+int lda_trainer_set_chunk_range(lda_trainer* t, int32_t first, int32_t last);
+/* Device address and length of the trainer's topic array (uint16, word-sorted), for a
+ * collective that exchanges topic slices in place between sweeps. */
+int lda_trainer_topics_device(lda_trainer* t, void** ptr, int64_t* count);
 
 /* n full sweeps of the driver loop EZLDA/mainKernel.cu:158-380 on resident
  * data; ll_mode=1 also evaluates the FP64 log-likelihood of every sweep.

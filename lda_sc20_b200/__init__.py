@@ -263,6 +263,16 @@ class Trainer:
         check(self._lib.lda_trainer_get_stream(self._h, C.byref(s)))
         return s.value or 0
 
+    def set_chunk_range(self, first: int, last: int) -> None:
+        """Sample (and rebuild doc rows for) chunks [first, last) only."""
+        check(self._lib.lda_trainer_set_chunk_range(self._h, first, last))
+
+    def topics_device(self) -> tuple[int, int]:
+        """(device address, length) of the uint16 topic array."""
+        p, n = C.c_void_p(), C.c_int64()
+        check(self._lib.lda_trainer_topics_device(self._h, C.byref(p), C.byref(n)))
+        return p.value or 0, n.value
+
     @property
     def device_bytes(self) -> int:
         b = C.c_int64()

@@ -95,6 +95,8 @@ SIGNATURES = {
     "lda_trainer_set_stream": (I32, [P, P]),
     "lda_trainer_get_stream": (I32, [P, C.POINTER(P)]),
     "lda_trainer_device_bytes": (I32, [P, C.POINTER(I64)]),
+    "lda_trainer_set_chunk_range": (I32, [P, I32, I32]),
+    "lda_trainer_topics_device": (I32, [P, C.POINTER(P), C.POINTER(I64)]),
     "lda_trainer_iterate": (I32, [P, I32, I32]),
     "lda_iterate_host": (I32, [P, P, P, I32, C.POINTER(F64)]),
     "lda_trainer_loglik": (I32, [P, C.POINTER(F64), C.POINTER(I64)]),

@@ -81,6 +81,7 @@ int main(int argc, char** argv) {
     lda_trainer_get_iteration(tr, &it0);
     for (int it = 0; it < iters; ++it) {
         const int ll = ll_every > 0 && (it % ll_every == 0 || it == iters - 1);
+        lda_trainer_reset_stats(tr);
         auto t0 = std::chrono::steady_clock::now();
         if (lda_trainer_iterate(tr, 1, ll) != LDA_OK) return die("sweep");
         auto t1 = std::chrono::steady_clock::now();

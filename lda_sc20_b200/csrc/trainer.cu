@@ -78,6 +78,9 @@ struct lda_trainer {
     int64_t last_ll_tokens = 0;
     bool ll_valid = false;
     std::vector<bool> chunk_sampled_ll;
+    int chunk_first = 0, chunk_last = 0;  // sampled chunk range of lda_trainer_iterate
+
+    int64_t range_tokens() const { return chunk_tok[chunk_last] - chunk_tok[chunk_first]; }
 
     ~lda_trainer() {
         if (device >= 0) cudaSetDevice(device);
@@ -308,6 +311,8 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
     CUDA_TRY(cudaDeviceSynchronize());
     T.chunk_sampled_ll.assign(T.C, false);
+    T.chunk_first = 0;
+    T.chunk_last = T.C;
     *out = t.release();
     return LDA_OK;
 }
@@ -326,6 +331,23 @@ extern "C" int lda_trainer_set_stream(lda_trainer* t, void* s) {
 extern "C" int lda_trainer_get_stream(lda_trainer* t, void** s) {
     if (!t || !s) return fail(LDA_ERR_ARG, "null argument");
     *s = (void*)t->stream;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_set_chunk_range(lda_trainer* t, int32_t first, int32_t last) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (first < 0 || last > t->C || first >= last)
+        return fail(LDA_ERR_ARG, "chunk range [%d, %d) outside [0, %d)", first, last, t->C);
+    t->chunk_first = first;
+    t->chunk_last = last;
+    t->ll_valid = false;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_topics_device(lda_trainer* t, void** ptr, int64_t* count) {
+    if (!t || !ptr) return fail(LDA_ERR_ARG, "null argument");
+    *ptr = (void*)t->z;
+    if (count) *count = t->N;
     return LDA_OK;
 }
 
@@ -420,8 +442,8 @@ extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) 
 
 static int perplexity_async(lda_trainer* t) {
     t->begin_stage(4);
-    const int n = t->s_tile_base[t->C];
-    dev::k_ll_reduce<<<1, 1024, 0, t->stream>>>(t->tile_ll, n, t->ll_dev);
+    const int base = t->s_tile_base[t->chunk_first], n = t->s_tile_base[t->chunk_last] - base;
+    dev::k_ll_reduce<<<1, 1024, 0, t->stream>>>(t->tile_ll + base, n, t->ll_dev);
     CUDA_TRY(cudaGetLastError());
     t->end_stage();
     CUDA_TRY(cudaMemcpyAsync(t->ll_host, t->ll_dev, sizeof(double), cudaMemcpyDeviceToHost, t->stream));
@@ -442,14 +464,14 @@ static int finish(lda_trainer* t) {
 
 extern "C" int lda_perplexity(lda_trainer* t, double* ll_sum) {
     if (!t) return fail(LDA_ERR_ARG, "null trainer");
-    for (int ch = 0; ch < t->C; ++ch)
+    for (int ch = t->chunk_first; ch < t->chunk_last; ++ch)
         if (!t->chunk_sampled_ll[ch]) return fail(LDA_ERR_STATE, "chunk %d was not sampled with ll_mode=1", ch);
     CUDA_TRY(cudaSetDevice(t->device));
     int rc = perplexity_async(t);
     if (rc) return rc;
     if ((rc = finish(t))) return rc;
     t->last_ll = *t->ll_host;
-    t->last_ll_tokens = t->N;
+    t->last_ll_tokens = t->range_tokens();
     t->ll_valid = true;
     if (ll_sum) *ll_sum = t->last_ll;
     return LDA_OK;
@@ -471,7 +493,7 @@ static int sweep_async(lda_trainer* t, int ll_mode) {
     int rc;
     if ((rc = lda_update_wt(t))) return rc;
     if ((rc = lda_max_topic(t))) return rc;
-    for (int ch = 0; ch < t->C; ++ch) {
+    for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
         if ((rc = lda_update_dt(t, ch))) return rc;
         if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
     }
@@ -484,7 +506,6 @@ extern "C" int lda_trainer_iterate(lda_trainer* t, int32_t n, int32_t ll_mode) {
     if (!t) return fail(LDA_ERR_ARG, "null trainer");
     if (n < 0) return fail(LDA_ERR_ARG, "negative iteration count");
     CUDA_TRY(cudaSetDevice(t->device));
-    CUDA_TRY(cudaMemsetAsync(t->ctr, 0, sizeof(unsigned long long) * kCounters, t->stream));
     for (int i = 0; i < n; ++i) {
         int rc = sweep_async(t, ll_mode);
         if (rc) return rc;
@@ -493,7 +514,7 @@ extern "C" int lda_trainer_iterate(lda_trainer* t, int32_t n, int32_t ll_mode) {
     if (rc) return rc;
     if (ll_mode && n > 0) {
         t->last_ll = *t->ll_host;
-        t->last_ll_tokens = t->N;
+        t->last_ll_tokens = t->range_tokens();
         t->ll_valid = true;
     }
     return LDA_OK;
@@ -513,7 +534,7 @@ extern "C" int lda_iterate_host(lda_trainer* t, const uint16_t* zin, uint16_t* z
     if ((rc = finish(t))) return rc;
     if (ll_mode) {
         t->last_ll = *t->ll_host;
-        t->last_ll_tokens = t->N;
+        t->last_ll_tokens = t->range_tokens();
         t->ll_valid = true;
         if (ll_sum) *ll_sum = t->last_ll;
     }
