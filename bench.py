@@ -52,6 +52,11 @@ def parse_args():
     p.add_argument("--chunks", type=int, default=0, help="override the preset's chunk count")
     p.add_argument("--sharded", action="store_true",
                    help="use the document-sharded path even on one GPU (it is the default for N>1)")
+    p.add_argument("--serve", action="store_true",
+                   help="fold-in serving benchmark instead of the training sweep")
+    p.add_argument("--serve-sweeps", type=int, default=30)
+    p.add_argument("--serve-rates", default="2000,10000,50000", help="offered loads in docs/s")
+    p.add_argument("--serve-seconds", type=float, default=1.5, help="arrival window per offered load")
     return p.parse_args()
 
 
@@ -502,9 +507,99 @@ def run_reference(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args, local):
+    """Fold-in serving against the word side of the K=1024 corpus trained for 100 sweeps.
+
+    Requests are new documents from the corpus' generative process (its topic-word
+    distributions, fresh theta), lengths lognormal(median 150, sigma 1.0) clipped to
+    [5, 4000]; each runs the configured sweeps (default 30) and returns theta as FP32[K].
+    Measured: one request at a time (max_active=1, closed loop), a saturated batch (all
+    requests queued at once), and real-time replays of seeded Poisson arrivals at the
+    offered loads with p50/p99 latency from scheduled arrival to theta on the host."""
+    import numpy as np
+    import torch
+    import lda_sc20_b200 as L
+    from lda_sc20_b200.serving import Model, Server
+
+    torch.cuda.set_device(local)
+    corpus = make_corpus("c1", 0)
+    info = corpus.info
+    K = info.K_hint
+    tr = L.Trainer(corpus, K=K, seed=42, device=local)
+    tr.iterate(100)
+    model = Model(tr)
+    tr.close()
+    sweeps, seed = args.serve_sweeps, 7
+    rng = np.random.default_rng(11)
+    req_seed = [1000]
+
+    def requests(n):
+        req_seed[0] += 1
+        off, words = corpus.generate_requests(n, req_seed[0])
+        return off, words, [words[off[i]:off[i + 1]] for i in range(n)]
+
+    clocks = ClockSampler(physical_gpu(local))
+    clocks.start()
+    # one request at a time
+    single = Server(model, sweeps=sweeps, max_active=1, max_tokens=1 << 16, seed=seed)
+    _, _, docs1 = requests(300)
+    single.run(docs1[:20])
+    t0 = time.perf_counter()
+    single.run(docs1)
+    single_dps = len(docs1) / (time.perf_counter() - t0)
+    single.close()
+    # saturated batch
+    batch = Server(model, sweeps=sweeps, max_active=16384, max_tokens=1 << 24, seed=seed)
+    _, _, docsb = requests(60000)
+    batch.run(docsb[:4000])
+    s0, l0 = batch.stats()
+    t0 = time.perf_counter()
+    th_batch = batch.run(docsb)
+    batch_s = time.perf_counter() - t0
+    s1, l1 = batch.stats()
+    batch_dps = len(docsb) / batch_s
+    tokens_b = int(sum(len(d) for d in docsb))
+    batch.close()
+    # 32 of the batch's requests again, one at a time with the same request ids
+    alone = Server(model, sweeps=sweeps, max_active=1, max_tokens=1 << 16, seed=seed)
+    ident = 0
+    for i in range(32):
+        alone.submit(i, docsb[i])
+        while (r := alone.poll()) is None:
+            alone.step()
+        ident += int(np.array_equal(r[1].view(np.uint32), th_batch[i].view(np.uint32)))
+    alone.close()
+    rates = []
+    for rate in [float(x) for x in args.serve_rates.split(",") if x]:
+        n = max(1, int(rate * args.serve_seconds))
+        off, words, _ = requests(n)
+        arrival = np.cumsum(rng.exponential(1.0 / rate, size=n))
+        arrival -= arrival[0]
+        srv = Server(model, sweeps=sweeps, max_active=16384, max_tokens=1 << 24, seed=seed)
+        lat, _, wall = srv.replay(off, words, arrival)
+        srv.close()
+        rates.append({"offered_docs_per_s": rate, "requests": n, "achieved_docs_per_s": n / wall,
+                      "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+                      "max_ms": float(lat.max() * 1e3)})
+    ck = clocks.stop()
+    line = {"metric": "foldin_docs_per_s", "value": batch_dps, "unit": "docs/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"fold-in against the K={K} V={info.vocab} lognormal corpus trained 100 sweeps; "
+                                   f"new documents from its generative process, lengths lognormal(median 150, "
+                                   f"sigma 1.0) in [5,4000]; {sweeps} sweeps per request; theta FP32[K]",
+                       "sweeps": sweeps, "K": K, "V": int(info.vocab)},
+            "one_at_a_time_docs_per_s": single_dps, "batch_vs_one_at_a_time": batch_dps / single_dps,
+            "batch_token_sweeps_per_s": tokens_b * sweeps / batch_s,
+            "batch_steps": s1 - s0, "gpu_launches": l1 - l0,
+            "alone_equals_batched": f"{ident}/32", "rates": rates, "clocks": ck}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
+    if args.serve:
+        return run_serving(args, local)
     if args.impl == "reference":
         run_reference(args, world, rank, local)
     else:

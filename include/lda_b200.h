@@ -88,6 +88,14 @@ enum {
 };
 
 int lda_corpus_generate(const lda_gen_config* cfg, lda_corpus** out);
+/* New documents from the generative process of a generated corpus (no counterpart in the
+ * reference): its topic-word distributions, fresh theta ~ Dir(theta_conc), lengths
+ * lognormal(len_mu, len_sigma) clipped to [len_min, len_max], all from request_seed;
+ * words are the corpus' frequency ranks.  doc_off gets n+1 offsets; with words NULL only
+ * the offsets are drawn (sizing call), else words needs doc_off[n] <= cap entries. */
+int lda_corpus_generate_requests(const lda_corpus* c, uint64_t request_seed, int64_t n, double len_mu,
+                                 double len_sigma, int32_t len_min, int32_t len_max, int64_t* doc_off,
+                                 int32_t* words, int64_t cap);
 /* Reads an EZLDA chunk directory (lengthVec.txt, docLength.txt, TLLength.txt,
  * TLSplit.txt, chunk<c>/{TL,word2DocMap,wordCountOffset,docCountOffset}.txt),
  * replacing Document::loadDocument / DocChunk::loadChunk (EZLDA/Doc.cu:45-108,
@@ -279,6 +287,54 @@ typedef struct {
  * different streams or devices sharing a context) race; serialise them.  The call is
  * asynchronous on `stream` (NULL: the legacy default stream) and sets `device` current. */
 int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream);
+
+/* ------------------------------------------------ fold-in serving */
+/* No counterpart in the reference: EZLDA trains only.  A model is the frozen word side
+ * of a trainer (phi_wk = (n_wk+beta)/(n_k+V*beta) as a dense [V][K] float matrix plus
+ * the per-word max topics and Q partials); fold-in of a new document runs `sweeps`
+ * sweeps of the training sampler with the word side frozen and returns
+ * theta_k = (n_dk+alpha)/(len+K*alpha).  A request's randoms are keyed on
+ * (server seed, request id, sweep, token position): the same request gives the same
+ * topics and theta whatever it is batched with. */
+typedef struct lda_model lda_model;
+typedef struct lda_server lda_server;
+
+/* Freezes the trainer's current topics into a model (rebuilds the word-topic counts and
+ * the per-word statistics first).  device_budget > 0 bounds the model's bytes. */
+int lda_model_from_trainer(lda_trainer* t, int64_t device_budget, lda_model** out);
+int lda_model_info(const lda_model* m, int32_t* K, int64_t* V, int64_t* bytes);
+int lda_model_get_phi(const lda_model* m, int32_t w, float* out /*K*/);
+void lda_model_free(lda_model* m);
+
+/* A continuous-batching server over one model: a token pool of max_tokens tokens
+ * (0: a quarter of the free device memory), at most max_active requests in flight.
+ * The model must outlive the server. */
+int lda_server_create(lda_model* m, int64_t max_tokens, int32_t max_active, int32_t sweeps, uint64_t seed,
+                      lda_server** out);
+int lda_server_destroy(lda_server* s);
+/* Queues a document (word ranks of the model's vocabulary, 1..65535 tokens). */
+int lda_server_submit(lda_server* s, uint32_t rid, const int32_t* words, int32_t len);
+/* One step: admits queued requests that fit (FIFO), queues one sweep of every active
+ * request on the server's stream, and retires requests whose last sweep has completed.
+ * Up to two steps are queued on the device before a step waits for the older one; with
+ * nothing to issue, a step waits for every queued step.  *n_done = requests retired. */
+int lda_server_step(lda_server* s, int32_t* n_done);
+/* Pops one finished request: returns 1 and fills rid / theta (K floats) / latency
+ * (seconds from submit to completion), or 0 when none is waiting. */
+int lda_server_poll(lda_server* s, uint32_t* rid, float* theta, double* latency_s);
+int lda_server_status(const lda_server* s, int32_t* queued, int32_t* active, int64_t* free_tokens);
+/* Current topics of an active request (len must match; synchronises the server's stream). */
+int lda_server_get_topics(lda_server* s, uint32_t rid, uint16_t* out, int32_t len);
+/* Tokens per work item (a multiple of 32, default 32): a request is split into items of
+ * this many tokens, each sampled by one warp.  Only while the server is idle. */
+int lda_server_set_item_tokens(lda_server* s, int32_t n);
+/* Steps issued and fold-in kernel launches since creation. */
+int lda_server_stats(const lda_server* s, int64_t* steps, int64_t* kernel_launches);
+/* Real-time replay on an idle server: document i (words[doc_off[i]..doc_off[i+1]))
+ * arrives arrival_s[i] seconds after the start (non-decreasing) and gets request id i;
+ * latency_s[i] = completion - scheduled arrival; theta (n x K) optional. */
+int lda_serve_replay(lda_server* s, int32_t n, const int64_t* doc_off, const int32_t* words,
+                     const double* arrival_s, double* latency_s, float* theta, double* wall_s);
 
 #ifdef __cplusplus
 }

@@ -145,6 +145,20 @@ class Corpus:
         z = np.ascontiguousarray(z, dtype=np.uint16)
         check(self._lib.lda_corpus_set_topics(self._h, _ptr(z), len(z)))
 
+    def generate_requests(self, n: int, seed: int, len_median: float = 150.0, len_sigma: float = 1.0,
+                          len_min: int = 5, len_max: int = 4000) -> tuple[np.ndarray, np.ndarray]:
+        """n new documents from this generated corpus' process (its phi, fresh theta),
+        lognormal lengths with the given median and sigma clipped to [len_min, len_max]:
+        (doc_off[n+1], words) with words as this corpus' frequency ranks."""
+        off = np.zeros(n + 1, dtype=np.int64)
+        mu = math.log(len_median)
+        check(self._lib.lda_corpus_generate_requests(self._h, seed, n, mu, len_sigma, len_min, len_max,
+                                                     _ptr(off), None, 0))
+        words = np.empty(int(off[-1]), dtype=np.int32)
+        check(self._lib.lda_corpus_generate_requests(self._h, seed, n, mu, len_sigma, len_min, len_max,
+                                                     _ptr(off), _ptr(words), len(words)))
+        return off, words
+
 
 @dataclass
 class SweepStats:

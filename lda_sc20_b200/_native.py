@@ -124,6 +124,21 @@ SIGNATURES = {
     "lda_get_doc_rows": (I64, [P, P, P, I64]),
     "lda_get_token_meta": (I32, [P, P]),
     "lda_sample_chunk_noalloc": (I32, [C.POINTER(SampleIO), I32, P]),
+    "lda_model_from_trainer": (I32, [P, I64, P]),
+    "lda_model_info": (I32, [P, P, P, P]),
+    "lda_model_get_phi": (I32, [P, I32, P]),
+    "lda_model_free": (None, [P]),
+    "lda_server_create": (I32, [P, I64, I32, I32, U64, P]),
+    "lda_server_destroy": (I32, [P]),
+    "lda_server_submit": (I32, [P, U32, P, I32]),
+    "lda_server_step": (I32, [P, P]),
+    "lda_server_poll": (I32, [P, P, P, P]),
+    "lda_server_status": (I32, [P, P, P, P]),
+    "lda_server_get_topics": (I32, [P, U32, P, I32]),
+    "lda_corpus_generate_requests": (I32, [P, U64, I64, F64, F64, I32, I32, P, P, I64]),
+    "lda_server_set_item_tokens": (I32, [P, I32]),
+    "lda_server_stats": (I32, [P, P, P]),
+    "lda_serve_replay": (I32, [P, I32, P, P, P, P, P, P]),
 }
 
 _lib = None

@@ -33,6 +33,10 @@ struct lda_corpus {
     std::vector<int64_t> word_count; // [V]
     std::vector<int64_t> seg_off;    // [C*V]
     std::vector<int64_t> seg_cnt;    // [C*V]
+    // generated corpora: the generator configuration and raw word -> frequency rank
+    bool generated = false;
+    lda_gen_config gen{};
+    std::vector<int32_t> rank_of;    // [V]
 };
 
 namespace lda {
@@ -63,5 +67,19 @@ struct Philox {
 };
 
 uint16_t initial_topic(uint64_t seed, uint64_t tok, int32_t K);
+
+// Device arrays of a trainer that a frozen fold-in model is built from (trainer.cu).
+struct ModelSource {
+    int device = 0, K = 0, Vd = 0;
+    int64_t V = 0;
+    float alpha = 0, beta = 0;
+    const int* n_k = nullptr;
+    const int* dwt = nullptr;
+    const uint32_t *swt_off = nullptr, *swt_nnz = nullptr, *swt_ent = nullptr, *top2 = nullptr;
+    const void* phi4 = nullptr;  // float4 per word
+    const float* ql = nullptr;   // 32 per word
+    void* stream = nullptr;
+};
+int trainer_model_source(lda_trainer* t, ModelSource* out);
 
 }  // namespace lda

@@ -214,65 +214,87 @@ struct Alias {
 
 using namespace lda;
 
-extern "C" int lda_corpus_generate(const lda_gen_config* g, lda_corpus** out) {
-    if (!g || !out) return fail(LDA_ERR_ARG, "null argument");
-    *out = nullptr;
+namespace {
+
+int check_gen_config(const lda_gen_config* g) {
     if (g->num_docs <= 0 || g->vocab <= 0 || g->gen_topics <= 0 || g->len_min < 1 ||
         g->len_max < g->len_min || g->len_max > 65535 || g->theta_conc <= 0 || g->phi_conc <= 0 ||
         g->K < 1 || g->K > 65535 || g->num_chunks < 1 || g->num_chunks > g->num_docs)
         return fail(LDA_ERR_ARG, "lda_corpus_generate: invalid configuration");
     if (g->len_kind == 0 && (g->len_p1 <= 0 || g->len_p1 > 700))
         return fail(LDA_ERR_ARG, "Poisson mean must be in (0,700]");
-    const int64_t D = g->num_docs, V = g->vocab;
+    return LDA_OK;
+}
+
+int64_t draw_length(Rng& rng, int32_t kind, double p1, double p2, int32_t lo, int32_t hi) {
+    int64_t L;
+    if (kind == 0) L = rng.poisson(p1);
+    else L = (int64_t)std::llround(std::exp(p1 + p2 * rng.normal()));
+    return std::max<int64_t>(lo, std::min<int64_t>(hi, L));
+}
+
+// The generating topic-word distributions phi_t ~ Dir(a), one alias table per topic.
+std::vector<Alias> draw_phi(Rng& rng, const lda_gen_config* g) {
+    const int64_t V = g->vocab;
     const int32_t T = g->gen_topics;
+    std::vector<double> a(V);
+    if (g->phi_kind == 0) {
+        std::fill(a.begin(), a.end(), g->phi_conc);
+    } else {
+        double zs = 0.0;
+        for (int64_t r = 0; r < V; ++r) zs += std::pow((double)(r + 1), -g->phi_zipf_s);
+        for (int64_t r = 0; r < V; ++r) a[r] = g->phi_conc * (double)V * std::pow((double)(r + 1), -g->phi_zipf_s) / zs;
+    }
+    std::vector<Alias> phi(T);
+    std::vector<double> lg(V), p(V);
+    for (int32_t t = 0; t < T; ++t) {
+        double mx = -INFINITY;
+        for (int64_t v = 0; v < V; ++v) { lg[v] = rng.log_gamma_draw(a[v]); mx = std::max(mx, lg[v]); }
+        double s = 0.0;
+        for (int64_t v = 0; v < V; ++v) { p[v] = std::exp(lg[v] - mx); s += p[v]; }
+        for (int64_t v = 0; v < V; ++v) p[v] /= s;
+        phi[t].build(p);
+    }
+    return phi;
+}
+
+// Tokens of one document of length L: topics by the Polya urn of theta ~ Dir(theta_conc),
+// words from phi.
+void draw_doc(Rng& rng, const std::vector<Alias>& phi, double theta_conc, int64_t L, std::vector<int32_t>& tt,
+              int32_t* out) {
+    const int32_t T = (int32_t)phi.size();
+    const double Ta = (double)T * theta_conc;
+    tt.resize(L);
+    for (int64_t i = 0; i < L; ++i) {
+        const double x = rng.u01() * ((double)i + Ta);
+        int32_t t;
+        if (x < (double)i) t = tt[(int64_t)x];
+        else t = std::min<int32_t>(T - 1, (int32_t)((x - (double)i) / theta_conc));
+        tt[i] = t;
+        out[i] = phi[t].draw(rng.u01());
+    }
+}
+
+}  // namespace
+
+extern "C" int lda_corpus_generate(const lda_gen_config* g, lda_corpus** out) {
+    if (!g || !out) return fail(LDA_ERR_ARG, "null argument");
+    *out = nullptr;
+    int rc = check_gen_config(g);
+    if (rc) return rc;
+    const int64_t D = g->num_docs, V = g->vocab;
     try {
         Rng rng(g->corpus_seed);
         // 1. doc lengths
         std::vector<int64_t> doc_off(D + 1, 0);
-        for (int64_t d = 0; d < D; ++d) {
-            int64_t L;
-            if (g->len_kind == 0) L = rng.poisson(g->len_p1);
-            else L = (int64_t)std::llround(std::exp(g->len_p1 + g->len_p2 * rng.normal()));
-            L = std::max<int64_t>(g->len_min, std::min<int64_t>(g->len_max, L));
-            doc_off[d + 1] = doc_off[d] + L;
-        }
+        for (int64_t d = 0; d < D; ++d)
+            doc_off[d + 1] = doc_off[d] + draw_length(rng, g->len_kind, g->len_p1, g->len_p2, g->len_min, g->len_max);
         const int64_t N = doc_off[D];
-        // 2. topic-word distributions phi_t ~ Dir(a)
-        std::vector<double> a(V);
-        if (g->phi_kind == 0) {
-            std::fill(a.begin(), a.end(), g->phi_conc);
-        } else {
-            double zs = 0.0;
-            for (int64_t r = 0; r < V; ++r) zs += std::pow((double)(r + 1), -g->phi_zipf_s);
-            for (int64_t r = 0; r < V; ++r)
-                a[r] = g->phi_conc * (double)V * std::pow((double)(r + 1), -g->phi_zipf_s) / zs;
-        }
-        std::vector<Alias> phi(T);
-        std::vector<double> lg(V), p(V);
-        for (int32_t t = 0; t < T; ++t) {
-            double mx = -INFINITY;
-            for (int64_t v = 0; v < V; ++v) { lg[v] = rng.log_gamma_draw(a[v]); mx = std::max(mx, lg[v]); }
-            double s = 0.0;
-            for (int64_t v = 0; v < V; ++v) { p[v] = std::exp(lg[v] - mx); s += p[v]; }
-            for (int64_t v = 0; v < V; ++v) p[v] /= s;
-            phi[t].build(p);
-        }
-        // 3. tokens: topics by the Polya urn of theta_d ~ Dir(theta_conc), words from phi
-        std::vector<int32_t> raw(N);
-        std::vector<int32_t> tt;
-        const double Ta = (double)T * g->theta_conc;
-        for (int64_t d = 0; d < D; ++d) {
-            const int64_t L = doc_off[d + 1] - doc_off[d];
-            tt.resize(L);
-            for (int64_t i = 0; i < L; ++i) {
-                const double x = rng.u01() * ((double)i + Ta);
-                int32_t t;
-                if (x < (double)i) t = tt[(int64_t)x];
-                else t = std::min<int32_t>(T - 1, (int32_t)((x - (double)i) / g->theta_conc));
-                tt[i] = t;
-                raw[doc_off[d] + i] = phi[t].draw(rng.u01());
-            }
-        }
+        // 2. topic-word distributions
+        std::vector<Alias> phi = draw_phi(rng, g);
+        // 3. tokens
+        std::vector<int32_t> raw(N), tt;
+        for (int64_t d = 0; d < D; ++d) draw_doc(rng, phi, g->theta_conc, doc_off[d + 1] - doc_off[d], tt, raw.data() + doc_off[d]);
         phi.clear();
         phi.shrink_to_fit();
         // 4. frequency ranks, dense split, layout
@@ -285,13 +307,48 @@ extern "C" int lda_corpus_generate(const lda_gen_config* g, lda_corpus** out) {
         for (int64_t j = 0; j < N; ++j) raw[j] = rank_of[raw[j]];
         const int32_t Vd = dense_count(sorted, g->K, g->dense_kind, g->dense_param);
         auto* c = new lda_corpus();
-        int rc = build_layout(*c, D, doc_off.data(), raw.data(), V, Vd, nullptr, g->K, g->num_chunks,
-                              g->topic_seed);
+        rc = build_layout(*c, D, doc_off.data(), raw.data(), V, Vd, nullptr, g->K, g->num_chunks, g->topic_seed);
         if (rc != LDA_OK) { delete c; return rc; }
+        c->generated = true;
+        c->gen = *g;
+        c->rank_of = std::move(rank_of);
         *out = c;
         return LDA_OK;
     } catch (const std::bad_alloc&) {
         return fail(LDA_ERR_NOMEM, "host allocation failed while generating the corpus");
+    }
+}
+
+extern "C" int lda_corpus_generate_requests(const lda_corpus* c, uint64_t request_seed, int64_t n, double len_mu,
+                                            double len_sigma, int32_t len_min, int32_t len_max, int64_t* doc_off,
+                                            int32_t* words, int64_t cap) {
+    if (!c || !doc_off || n < 0) return fail(LDA_ERR_ARG, "null argument");
+    if (!c->generated) return fail(LDA_ERR_STATE, "the corpus was not made by lda_corpus_generate");
+    if (len_min < 1 || len_max < len_min || len_max > 65535 || len_sigma < 0)
+        return fail(LDA_ERR_ARG, "request lengths must satisfy 1 <= len_min <= len_max <= 65535");
+    try {
+        // lengths from their own stream, so that the sizing call draws nothing else
+        Rng lrng(request_seed ^ 0x4C454E47544853ull);
+        doc_off[0] = 0;
+        for (int64_t i = 0; i < n; ++i) doc_off[i + 1] = doc_off[i] + draw_length(lrng, 1, len_mu, len_sigma, len_min, len_max);
+        if (!words) return LDA_OK;
+        if (cap < doc_off[n]) return fail(LDA_ERR_ARG, "words holds %lld entries, %lld needed", (long long)cap, (long long)doc_off[n]);
+        // the corpus' generating phi: replay its stream through the doc lengths
+        const lda_gen_config* g = &c->gen;
+        Rng rng(g->corpus_seed);
+        for (int64_t d = 0; d < g->num_docs; ++d) draw_length(rng, g->len_kind, g->len_p1, g->len_p2, g->len_min, g->len_max);
+        const std::vector<Alias> phi = draw_phi(rng, g);
+        Rng drng(request_seed);
+        std::vector<int32_t> tt;
+        for (int64_t i = 0; i < n; ++i) {
+            int32_t* w = words + doc_off[i];
+            const int64_t L = doc_off[i + 1] - doc_off[i];
+            draw_doc(drng, phi, g->theta_conc, L, tt, w);
+            for (int64_t j = 0; j < L; ++j) w[j] = c->rank_of[w[j]];
+        }
+        return LDA_OK;
+    } catch (const std::bad_alloc&) {
+        return fail(LDA_ERR_NOMEM, "host allocation failed while generating requests");
     }
 }
 

@@ -1,0 +1,177 @@
+// device_common.cuh -- device helpers shared by the sweep and the fold-in kernels.
+//
+// Every float operation is an explicit round-to-nearest intrinsic, so the compiler cannot
+// contract or reorder it; the summation orders below are part of the arithmetic
+// specification the CPU oracle restates.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace lda {
+namespace dev {
+
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float u2f(uint32_t x) { return __uint2float_rn(x); }
+
+// Inclusive Kogge-Stone scan over the warp: round `off` adds lane l-off into lane l.
+__device__ __forceinline__ float warp_ks_scan(float v, int lane) {
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const float t = __shfl_up_sync(FULL, v, off);
+        if (lane >= off) v = fadd(v, t);
+    }
+    return v;
+}
+
+// Philox4x32-10 (Salmon et al., SC'11), first output word.
+__device__ __forceinline__ uint32_t philox_x0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+        const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+        c1 = lo1;
+        c3 = lo0;
+        c0 = n0;
+        c2 = n2;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    return c0;
+}
+
+// u in [0,1) of token `tok` at sweep `iter` (replaces curand_uniform()/1.00001,
+// EZLDA/utility.cu:1353).
+__device__ __forceinline__ float token_uniform(uint32_t seed_lo, uint32_t seed_hi, uint32_t iter,
+                                               uint32_t tok) {
+    const uint32_t x = philox_x0(tok, 0u, iter, 0x4C444131u, seed_lo, seed_hi);
+    return u2f(x >> 8) * 0x1p-24f;
+}
+
+__device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uint32_t start, uint32_t cnt,
+                                             uint32_t* hist, int K, int lane, int* err) {
+    for (uint32_t base = 0; base < cnt; base += 32) {
+        const uint32_t i = base + lane;
+        bool valid = i < cnt;
+        uint32_t k = valid ? (uint32_t)__ldg(z + start + i) : 0xffffffffu;
+        if (valid && k >= (uint32_t)K) {
+            atomicOr(err, 1);
+            valid = false;
+            k = 0xfffffffeu;
+        }
+        const unsigned m = __match_any_sync(FULL, k);
+        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+    }
+}
+
+// ------------------------------------------------------------ word columns
+// phi_k = ((float)n_wk + beta) * r_k into a warp-private shared row (EZLDA builds the
+// same column as WTHead, utility.cu:1257-1269 sparse, :1698-1702 dense).
+__device__ __forceinline__ void build_column(float* col, const float* r, int w, int Vd, int K, float beta,
+                                             const int* __restrict__ dwt, const uint32_t* __restrict__ swt_off,
+                                             const uint32_t* __restrict__ swt_nnz,
+                                             const uint32_t* __restrict__ swt_ent, int lane, uint32_t* nnz_read) {
+    if (w < Vd) {
+        const int* row = dwt + (size_t)w * K;
+        for (int k = lane; k < K; k += 32) col[k] = fmul(fadd(__int2float_rn(__ldg(row + k)), beta), r[k]);
+    } else {
+        for (int k = lane; k < K; k += 32) col[k] = fmul(beta, r[k]);
+        __syncwarp();
+        const int s = w - Vd;
+        const uint32_t off = __ldg(swt_off + s), nnz = __ldg(swt_nnz + s);
+        for (uint32_t e = lane; e < nnz; e += 32) {
+            const uint32_t en = __ldg(swt_ent + off + e);
+            const uint32_t k = en >> 16;
+            col[k] = fmul(fadd(u2f(en & 0xffffu), beta), r[k]);
+        }
+        if (nnz_read && lane == 0) *nnz_read += nnz;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void warp_argmax(float& v, int& k) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        const float ov = __shfl_xor_sync(FULL, v, off);
+        const int ok = __shfl_xor_sync(FULL, k, off);
+        if (ov > v || (ov == v && ok < k)) {
+            v = ov;
+            k = ok;
+        }
+    }
+}
+
+__device__ __forceinline__ void fill_recip(float* r, const int* __restrict__ n_k, int K, float Vbeta) {
+    for (int k = threadIdx.x; k < K; k += blockDim.x) r[k] = __fdiv_rn(1.0f, fadd(__int2float_rn(n_k[k]), Vbeta));
+}
+
+// Second-level search over 32-entry rounds: term = weight of slot i, ok = slot may be
+// drawn; returns the key of the first ok slot whose carried scan exceeds t2, else the
+// last ok slot's key, else `fallback`.  Uniform across the warp.
+template <class Slot>
+__device__ __forceinline__ int warp_level2(uint32_t n, float t2, int fallback, int lane, Slot slot) {
+    float carry = 0.0f;
+    int last = -1;
+    for (uint32_t base = 0; base < n; base += 32) {
+        int key = -1;
+        float term = 0.0f;
+        bool ok = false;
+        if (base + lane < n) slot(base + lane, key, term, ok);
+        const float P = fadd(carry, warp_ks_scan(term, lane));
+        const unsigned f = __ballot_sync(FULL, ok && t2 < P);
+        const unsigned v = __ballot_sync(FULL, ok);
+        if (f) return __shfl_sync(FULL, key, __ffs(f) - 1);
+        if (v) last = __shfl_sync(FULL, key, 31 - __clz(v));
+        carry = __shfl_sync(FULL, P, 31);
+    }
+    return last >= 0 ? last : fallback;
+}
+
+// Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
+// loads of two entries are issued together).
+__device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
+                                            const float* col) {
+    float acc = 0.0f;
+    uint32_t q = b0;
+    for (; q + 2 <= b1; q += 2) {
+        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 1);
+        acc = ffma(u2f(e0 & 0xffffu), col[e0 >> 16], acc);
+        acc = ffma(u2f(e1 & 0xffffu), col[e1 >> 16], acc);
+    }
+    if (q < b1) {
+        const uint32_t e = __ldg(row + q);
+        acc = ffma(u2f(e & 0xffffu), col[e >> 16], acc);
+    }
+    return acc;
+}
+
+// The S-bucket draw inside one lane block: the block's serial partial sums (the same
+// fmaf chain as block_mass) are compared with t2; the first entry with colz > 0 whose
+// partial sum exceeds t2 wins, else the last entry with colz > 0, else `fallback`.
+__device__ __forceinline__ int block_draw(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
+                                          const float* col, float t2, int fallback) {
+    float acc = 0.0f;
+    int last = -1;
+    for (uint32_t q = b0; q < b1; ++q) {
+        const uint32_t e = __ldg(row + q);
+        const int k = (int)(e >> 16);
+        const float cz = col[k];
+        acc = ffma(u2f(e & 0xffffu), cz, acc);
+        if (cz > 0.0f) {
+            last = k;
+            if (t2 < acc) return k;
+        }
+    }
+    return last >= 0 ? last : fallback;
+}
+
+
+}  // namespace dev
+}  // namespace lda

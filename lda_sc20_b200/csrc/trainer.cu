@@ -669,6 +669,26 @@ extern "C" int lda_trainer_restore(lda_trainer* t, const char* path) {
 
 // ---------------------------------------------------------------- readback
 
+int lda::trainer_model_source(lda_trainer* t, ModelSource* o) {
+    if (!t || !o) return fail(LDA_ERR_ARG, "null argument");
+    o->device = t->device;
+    o->K = t->K;
+    o->Vd = t->Vd;
+    o->V = t->V;
+    o->alpha = t->alpha;
+    o->beta = t->beta;
+    o->n_k = t->n_k;
+    o->dwt = t->dwt;
+    o->swt_off = t->swt_off;
+    o->swt_nnz = t->swt_nnz;
+    o->swt_ent = t->swt_ent;
+    o->top2 = t->st_top2;
+    o->phi4 = t->st_phi;
+    o->ql = t->st_ql;
+    o->stream = t->stream;
+    return LDA_OK;
+}
+
 extern "C" int lda_get_topic_totals(lda_trainer* t, int32_t* nk) {
     if (!t || !nk) return fail(LDA_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(t->device));

@@ -54,6 +54,12 @@ def lib() -> C.CDLL:
         L.orc_sample.argtypes = [P, P, C.c_uint64, C.c_uint32, C.c_int32, C.c_int32, C.POINTER(SampleStats)]
         L.orc_iterate.argtypes = [P, P, C.c_uint64, C.c_uint32, C.c_int32, C.POINTER(SampleStats)]
         L.orc_token_probs.argtypes = [P, C.c_int64, P]
+        L.orc_foldin.argtypes = [P, P, C.c_int32, C.c_uint32, C.c_uint64, C.c_int32, P, P]
+        L.orc_foldin_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        L.orc_foldin_uniform.restype = C.c_float
+        L.orc_foldin_init.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int32]
+        L.orc_foldin_init.restype = C.c_uint16
+        L.orc_get_phi_row.argtypes = [P, C.c_int32, P]
         _lib = L
     return _lib
 
@@ -169,6 +175,21 @@ class Oracle:
         p = np.empty(self.K, dtype=np.float64)
         lib().orc_token_probs(self._h, tok, _p(p))
         return p
+
+    def foldin(self, words, rid: int, seed: int, sweeps: int):
+        """Fold-in of one document against the counts of the last rebuild: (topics, theta)."""
+        w = np.ascontiguousarray(words, dtype=np.int32)
+        z = np.empty(len(w), dtype=np.uint16)
+        th = np.empty(self.K, dtype=np.float32)
+        rc = lib().orc_foldin(self._h, _p(w), len(w), rid, seed, sweeps, _p(z), _p(th))
+        if rc:
+            raise ValueError(f"orc_foldin failed ({rc})")
+        return z, th
+
+    def phi_row(self, w: int):
+        a = np.empty(self.K, dtype=np.float32)
+        lib().orc_get_phi_row(self._h, w, _p(a))
+        return a
 
     @staticmethod
     def token_uniform(seed: int, it: int, tok: int) -> float:

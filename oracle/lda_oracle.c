@@ -473,9 +473,6 @@ typedef struct {
     float** fcol;
     double* wll;            /* per-word LL partial */
     orc_sample_stats* part; /* per-thread counters */
-    int32_t** key;          /* per-thread level-2 slots (K) */
-    float** term;
-    int** ok;
 } sp_ctx;
 
 /* Bucket search shared by S and Q (EZLDA/utility.cu:1456-1552): first lane
@@ -486,47 +483,131 @@ static int pick_lane(float t, const float* P, const float* L) {
     return -1;
 }
 
-/* Second-level bucket search in rounds of 32 slots: each round's terms are
- * Kogge-Stone scanned and offset by the carried total of the previous rounds; the
- * first slot that may be drawn (ok) with t2 < prefix wins, else the last ok slot. */
-static int32_t level2(int32_t n, const float* term, const int* ok, const int32_t* key, float t2,
-                      int32_t fallback) {
+/* The per-word state a draw reads. */
+typedef struct {
+    int32_t K, maxK;
+    float alpha, phi1, phi2, phi3, Q;
+    const float* QL;   /* 32 lane partials of Q */
+    const float* QP;   /* their Kogge-Stone scan */
+    const float* colz; /* the word's column with colz[maxK] = 0 */
+} word_ctx;
+
+enum { BR_MAX = 0, BR_S = 1, BR_Q = 2 };
+
+/* One token's draw under the arithmetic specification at the top of this file.  The
+ * doc row (ascending k), the counts of the word's max / 2nd topic in the doc and the
+ * uniform are the token's inputs.  With force_eval the row mass is evaluated even when
+ * the early-accept bound settles the draw (LL mode).  *total is the full mass when the
+ * row was evaluated (else 0). */
+static int32_t draw_token(const word_ctx* w, const uint32_t* row, int32_t nnz, int32_t cmax, int32_t c2,
+                          int32_t nd, float u, int force_eval, int* ea_out, int* evaluated, float* total_out,
+                          int* branch) {
+    const float pmax = ((float)cmax + w->alpha) * w->phi1;
+    const int32_t rest = nd - cmax - c2;
+    const float shat = fmaf((float)c2, w->phi2, (float)rest * w->phi3);
+    const float bound = (pmax + shat) + w->Q;
+    const int ea = (u * bound < pmax);
+    *ea_out = ea;
+    *evaluated = 0;
+    *total_out = 0.0f;
+    *branch = BR_MAX;
+    if (ea && !force_eval) return w->maxK;
+    /* S: lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
+     * the lane sums are Kogge-Stone scanned (EZLDA sums the same row in 32-entry blocks,
+     * EZLDA/utility.cu:1376-1440) */
+    const int32_t B = (nnz + LANES - 1) / LANES;
+    float SL[LANES], SP[LANES];
+    for (int l = 0; l < LANES; ++l) {
+        float acc = 0.0f;
+        for (int32_t q = l * B; q < l * B + B && q < nnz; ++q)
+            acc = fmaf((float)(row[q] & 0xffffu), w->colz[row[q] >> 16], acc);
+        SL[l] = acc;
+    }
+    ks_scan32(SL, SP);
+    const float S = SP[LANES - 1];
+    const float pS = pmax + S;
+    const float total = pS + w->Q;
+    *evaluated = 1;
+    *total_out = total;
+    if (ea) return w->maxK;
+    const float target = u * total;
+    if (target < pmax) return w->maxK;
+    if (target < pS) {
+        *branch = BR_S;
+        const float tt = target - pmax;
+        const int l = pick_lane(tt, SP, SL);
+        const float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
+        if (l < 0) return w->maxK;
+        /* the block's serial partial sums (the fmaf chain of SL[l]) */
+        float acc = 0.0f;
+        int32_t last = -1;
+        for (int32_t q = l * B; q < l * B + B && q < nnz; ++q) {
+            const int32_t k = (int32_t)(row[q] >> 16);
+            acc = fmaf((float)(row[q] & 0xffffu), w->colz[k], acc);
+            if (w->colz[k] > 0.0f) {
+                last = k;
+                if (t2 < acc) return k;
+            }
+        }
+        return last >= 0 ? last : w->maxK;
+    }
+    *branch = BR_Q;
+    const float tt = target - pS;
+    const int l = pick_lane(tt, w->QP, w->QL);
+    const float t2 = tt - (l > 0 ? w->QP[l - 1] : 0.0f);
+    if (l < 0) return w->maxK;
+    /* rounds of 32 of the lane's topics k = l, l+32, ...: carry + Kogge-Stone scan */
+    const int32_t n = (w->K - l + LANES - 1) / LANES;
     float carry = 0.0f;
     int32_t last = -1;
     for (int32_t base = 0; base < n; base += LANES) {
         float tr[LANES], P[LANES];
-        for (int i = 0; i < LANES; ++i) tr[i] = base + i < n ? term[base + i] : 0.0f;
+        for (int i = 0; i < LANES; ++i) tr[i] = base + i < n ? w->alpha * w->colz[l + LANES * (base + i)] : 0.0f;
         ks_scan32(tr, P);
         for (int i = 0; i < LANES; ++i) P[i] = carry + P[i];
-        for (int i = 0; i < LANES && base + i < n; ++i)
-            if (ok[base + i] && t2 < P[i]) return key[base + i];
-        for (int i = 0; i < LANES && base + i < n; ++i)
-            if (ok[base + i]) last = key[base + i];
+        for (int i = 0; i < LANES && base + i < n; ++i) {
+            const int32_t k = l + LANES * (base + i);
+            if (w->colz[k] > 0.0f && t2 < P[i]) return k;
+        }
+        for (int i = 0; i < LANES && base + i < n; ++i) {
+            const int32_t k = l + LANES * (base + i);
+            if (w->colz[k] > 0.0f) last = k;
+        }
         carry = P[LANES - 1];
     }
-    return last >= 0 ? last : fallback;
+    return last >= 0 ? last : w->maxK;
+}
+
+/* Fills the word context of word w (its column with colz[maxK] = 0). */
+static void word_ctx_of(const orc_state* s, int32_t w, int32_t* cnt, float* colz, float* QP, word_ctx* wc) {
+    word_column(s, w, cnt, colz);
+    wc->K = s->K;
+    wc->alpha = s->alpha;
+    wc->maxK = (int32_t)(s->top2[w] & 0xffffu);
+    wc->phi1 = s->phi4[(int64_t)w * 4 + 0];
+    wc->phi2 = s->phi4[(int64_t)w * 4 + 1];
+    wc->phi3 = s->phi4[(int64_t)w * 4 + 2];
+    wc->QL = s->ql + (int64_t)w * LANES;
+    ks_scan32(wc->QL, QP);
+    wc->QP = QP;
+    wc->Q = QP[LANES - 1];
+    colz[wc->maxK] = 0.0f;
+    wc->colz = colz;
 }
 
 static void sp_words(void* c, int64_t b, int64_t e, int tid) {
     sp_ctx* x = (sp_ctx*)c;
     orc_state* s = x->s;
-    const int32_t K = s->K;
-    const float alpha = s->alpha;
-    const double den_add = (double)K * (double)alpha;
+    const double den_add = (double)s->K * (double)s->alpha;
     int32_t* cnt = x->icnt[tid];
     float* colz = x->fcol[tid];
     orc_sample_stats* st = &x->part[tid];
     for (int64_t w = b; w < e; ++w) {
         if (w % x->word_stride) continue;
         if (s->woff[w + 1] == s->woff[w]) continue;
-        word_column(s, (int32_t)w, cnt, colz);
-        const int32_t maxK = (int32_t)(s->top2[w] & 0xffffu);
-        const float phi1 = s->phi4[w * 4 + 0], phi2 = s->phi4[w * 4 + 1], phi3 = s->phi4[w * 4 + 2];
-        const float* QL = s->ql + w * LANES;
         float QP[LANES];
-        ks_scan32(QL, QP);
-        const float Q = QP[LANES - 1];
-        colz[maxK] = 0.0f;
+        word_ctx wc;
+        word_ctx_of(s, (int32_t)w, cnt, colz, QP, &wc);
         double wll = 0.0;
         for (int64_t j = s->woff[w]; j < s->woff[w + 1]; ++j) {
             const int64_t t = s->wtok[j];
@@ -534,82 +615,23 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
             const int32_t nd = (int32_t)(s->doff[d + 1] - s->doff[d]);
             const uint32_t* row = s->rent + s->rcap[d];
             const int32_t nnz = s->rnnz[d];
-            const int32_t cmax = row_count(row, nnz, maxK);
+            const int32_t cmax = row_count(row, nnz, wc.maxK);
             const int32_t c2 = row_count(row, nnz, (int32_t)(s->top2[w] >> 16));
             const float u = orc_token_uniform(x->seed, x->iter, (uint64_t)t);
-            const float pmax = ((float)cmax + alpha) * phi1;
-            const int32_t rest = nd - cmax - c2;
-            const float shat = fmaf((float)c2, phi2, (float)rest * phi3);
-            const float bound = (pmax + shat) + Q;
-            const int ea = (u * bound < pmax);
+            int ea, evald, br;
+            float total;
+            const int32_t z = draw_token(&wc, row, nnz, cmax, c2, nd, u, x->ll_mode, &ea, &evald, &total, &br);
             st->tokens++;
             if (ea) st->early_accept++;
-            if (ea && !x->ll_mode) { x->z_out[t] = (uint16_t)maxK; st->branch_max++; continue; }
-            /* S: lane l sums the contiguous block [l*B, l*B+B) of the doc row (ascending k),
-             * B = ceil(nnz/32); the lane sums are Kogge-Stone scanned (EZLDA sums the same
-             * row in 32-entry blocks, EZLDA/utility.cu:1376-1440) */
-            const int32_t B = (nnz + LANES - 1) / LANES;
-            float SL[LANES], SP[LANES];
-            for (int l = 0; l < LANES; ++l) {
-                float acc = 0.0f;
-                for (int32_t q = l * B; q < l * B + B && q < nnz; ++q)
-                    acc = fmaf((float)(row[q] & 0xffffu), colz[row[q] >> 16], acc);
-                SL[l] = acc;
+            if (evald) {
+                st->full++;
+                st->sum_nnz_full += nnz;
+                if (x->ll_mode) wll += log((double)total / ((double)nd + den_add));
             }
-            ks_scan32(SL, SP);
-            const float S = SP[LANES - 1];
-            const float pS = pmax + S;
-            const float total = pS + Q;
-            st->full++;
-            st->sum_nnz_full += nnz;
-            if (x->ll_mode) wll += log((double)total / ((double)nd + den_add));
-            if (ea) { x->z_out[t] = (uint16_t)maxK; st->branch_max++; continue; }
-            const float target = u * total;
-            int32_t znew;
-            if (target < pmax) {
-                znew = maxK;
-                st->branch_max++;
-            } else if (target < pS) {
-                const float tt = target - pmax;
-                const int l = pick_lane(tt, SP, SL);
-                const float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
-                znew = maxK;
-                if (l >= 0) {
-                    /* the block's serial partial sums (the fmaf chain of SL[l]) */
-                    float acc = 0.0f;
-                    int32_t found = -1, last = -1;
-                    for (int32_t q = l * B; q < l * B + B && q < nnz; ++q) {
-                        const int32_t k = (int32_t)(row[q] >> 16);
-                        acc = fmaf((float)(row[q] & 0xffffu), colz[k], acc);
-                        if (colz[k] > 0.0f) {
-                            last = k;
-                            if (t2 < acc) { found = k; break; }
-                        }
-                    }
-                    znew = found >= 0 ? found : (last >= 0 ? last : maxK);
-                }
-                st->branch_s++;
-            } else {
-                const float tt = target - pS;
-                const int l = pick_lane(tt, QP, QL);
-                const float t2 = tt - (l > 0 ? QP[l - 1] : 0.0f);
-                znew = maxK;
-                if (l >= 0) {
-                    int32_t* key = x->key[tid];
-                    float* term = x->term[tid];
-                    int* ok = x->ok[tid];
-                    const int32_t n = (K - l + LANES - 1) / LANES;
-                    for (int32_t i = 0; i < n; ++i) {
-                        const int32_t k = l + LANES * i;
-                        key[i] = k;
-                        term[i] = alpha * colz[k];
-                        ok[i] = colz[k] > 0.0f;
-                    }
-                    znew = level2(n, term, ok, key, t2, maxK);
-                }
-                st->branch_q++;
-            }
-            x->z_out[t] = (uint16_t)znew;
+            if (br == BR_S) st->branch_s++;
+            else if (br == BR_Q) st->branch_q++;
+            else st->branch_max++;
+            x->z_out[t] = (uint16_t)z;
         }
         x->wll[w] = wll;
     }
@@ -626,15 +648,9 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
     x.fcol = (float**)calloc((size_t)nt, sizeof(float*));
     x.part = (orc_sample_stats*)calloc((size_t)nt, sizeof(orc_sample_stats));
     x.wll = (double*)calloc((size_t)s->V, sizeof(double));
-    x.key = (int32_t**)calloc((size_t)nt, sizeof(int32_t*));
-    x.term = (float**)calloc((size_t)nt, sizeof(float*));
-    x.ok = (int**)calloc((size_t)nt, sizeof(int*));
     for (int t = 0; t < nt; ++t) {
         x.icnt[t] = (int32_t*)calloc((size_t)s->K, sizeof(int32_t));
         x.fcol[t] = (float*)calloc((size_t)s->K, sizeof(float));
-        x.key[t] = (int32_t*)calloc((size_t)s->K + LANES, sizeof(int32_t));
-        x.term[t] = (float*)calloc((size_t)s->K + LANES, sizeof(float));
-        x.ok[t] = (int*)calloc((size_t)s->K + LANES, sizeof(int));
     }
     parallel_for(nt, s->V, 16, sp_words, &x);
     orc_sample_stats tot;
@@ -647,10 +663,10 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
         tot.branch_max += x.part[t].branch_max;
         tot.branch_s += x.part[t].branch_s;
         tot.branch_q += x.part[t].branch_q;
-        free(x.icnt[t]); free(x.fcol[t]); free(x.key[t]); free(x.term[t]); free(x.ok[t]);
+        free(x.icnt[t]); free(x.fcol[t]);
     }
     for (int32_t w = 0; w < s->V; ++w) tot.loglik += x.wll[w];
-    free(x.icnt); free(x.fcol); free(x.part); free(x.wll); free(x.key); free(x.term); free(x.ok);
+    free(x.icnt); free(x.fcol); free(x.part); free(x.wll);
     if (st) *st = tot;
     return 0;
 }
@@ -669,4 +685,79 @@ int orc_iterate(orc_state* s, uint16_t* z, uint64_t seed, uint32_t iter, int32_t
     s->z = NULL;
     free(zin);
     return rc;
+}
+
+/* ------------------------------------------------------------------- fold-in */
+/* Fold-in of a new document against frozen counts (the word-topic counts and n_k of the
+ * last orc_rebuild stay fixed; only the document's own topic counts move).  Each sweep
+ * draws every token with draw_token() from the document's sweep-start counts, as the
+ * training sweep does (EZLDA's sampler with the word-topic side frozen). */
+float orc_foldin_uniform(uint64_t seed, uint32_t rid, uint32_t sweep, uint32_t pos) {
+    uint32_t ctr[4] = {pos, rid, sweep, 0x464F4C44u};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t x[4];
+    orc_philox4x32_10(ctr, key, x);
+    return (float)(x[0] >> 8) * 0x1p-24f;
+}
+
+uint16_t orc_foldin_init(uint64_t seed, uint32_t rid, uint32_t pos, int32_t K) {
+    uint32_t ctr[4] = {pos, rid, 0xFFFFFFFFu, 0x46494E49u};
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t x[4];
+    orc_philox4x32_10(ctr, key, x);
+    return (uint16_t)(((uint64_t)x[0] * (uint64_t)(uint32_t)K) >> 32);
+}
+
+int orc_foldin(const orc_state* s, const int32_t* words, int32_t len, uint32_t rid, uint64_t seed,
+               int32_t sweeps, uint16_t* z, float* theta) {
+    if (!s || !s->built || !words || !z || len < 1 || len > 65535 || sweeps < 0) return -1;
+    const int32_t K = s->K;
+    for (int32_t i = 0; i < len; ++i)
+        if (words[i] < 0 || words[i] >= s->V) return -2;
+    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)K);
+    int32_t* hist = (int32_t*)calloc((size_t)K, sizeof(int32_t));
+    float* colz = (float*)malloc(sizeof(float) * (size_t)K);
+    uint32_t* row = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)K);
+    uint16_t* zn = (uint16_t*)malloc(sizeof(uint16_t) * (size_t)len);
+    if (!cnt || !hist || !colz || !row || !zn) {
+        free(cnt); free(hist); free(colz); free(row); free(zn);
+        return -3;
+    }
+    for (int32_t i = 0; i < len; ++i) z[i] = orc_foldin_init(seed, rid, (uint32_t)i, K);
+    for (int32_t sw = 0; sw < sweeps; ++sw) {
+        memset(hist, 0, sizeof(int32_t) * (size_t)K);
+        for (int32_t i = 0; i < len; ++i) hist[z[i]]++;
+        int32_t nnz = 0;
+        for (int32_t k = 0; k < K; ++k)
+            if (hist[k]) row[nnz++] = ((uint32_t)k << 16) | (uint32_t)hist[k];
+        for (int32_t i = 0; i < len; ++i) {
+            float QP[LANES];
+            word_ctx wc;
+            word_ctx_of(s, words[i], cnt, colz, QP, &wc);
+            const int32_t cmax = hist[wc.maxK];
+            const int32_t c2 = hist[s->top2[words[i]] >> 16];
+            const float u = orc_foldin_uniform(seed, rid, (uint32_t)sw, (uint32_t)i);
+            int ea, evald, br;
+            float total;
+            zn[i] = (uint16_t)draw_token(&wc, row, nnz, cmax, c2, len, u, 0, &ea, &evald, &total, &br);
+        }
+        memcpy(z, zn, sizeof(uint16_t) * (size_t)len);
+    }
+    if (theta) {
+        memset(hist, 0, sizeof(int32_t) * (size_t)K);
+        for (int32_t i = 0; i < len; ++i) hist[z[i]]++;
+        const float den = (float)len + (float)K * s->alpha;
+        for (int32_t k = 0; k < K; ++k) theta[k] = ((float)hist[k] + s->alpha) / den;
+    }
+    free(cnt); free(hist); free(colz); free(row); free(zn);
+    return 0;
+}
+
+int orc_get_phi_row(const orc_state* s, int32_t w, float* out) {
+    if (!s || !s->built || w < 0 || w >= s->V) return -1;
+    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)s->K);
+    if (!cnt) return -3;
+    word_column(s, w, cnt, out);
+    free(cnt);
+    return 0;
 }

@@ -88,6 +88,16 @@ int orc_iterate(orc_state* s, uint16_t* z, uint64_t seed, uint32_t iter,
  * disagreements and for distribution tests. */
 int orc_token_probs(const orc_state* s, int64_t tok, double* p /*K*/);
 
+/* Fold-in of one new document (words of the trained vocabulary) against the frozen
+ * counts of the last orc_rebuild: `sweeps` sweeps from Philox initial topics keyed on
+ * (seed, rid), then theta_k = ((float)n_dk + alpha) / ((float)len + (float)K * alpha). */
+float orc_foldin_uniform(uint64_t seed, uint32_t rid, uint32_t sweep, uint32_t pos);
+uint16_t orc_foldin_init(uint64_t seed, uint32_t rid, uint32_t pos, int32_t K);
+int orc_foldin(const orc_state* s, const int32_t* words, int32_t len, uint32_t rid, uint64_t seed,
+               int32_t sweeps, uint16_t* z, float* theta /*K or NULL*/);
+/* phi_k of word w under the counts of the last orc_rebuild. */
+int orc_get_phi_row(const orc_state* s, int32_t w, float* out /*K*/);
+
 #ifdef __cplusplus
 }
 #endif

@@ -150,3 +150,26 @@ def test_from_docs_and_argument_checks():
         L.Corpus.generate(bad)
     with pytest.raises(LdaError):
         L.Corpus.generate(L.corpus_config("c0", K=70000))
+
+
+def test_generate_requests_follow_the_corpus_process():
+    """Held-out requests: deterministic per seed, lengths clipped, words drawn from the
+    corpus' own topic-word distributions (their frequencies track the corpus ranks)."""
+    import math
+    c = L.Corpus.generate(L.corpus_config("c0"))
+    off, w = c.generate_requests(3000, seed=9, len_median=150, len_sigma=1.0, len_min=5, len_max=400)
+    off2, w2 = c.generate_requests(3000, seed=9, len_median=150, len_sigma=1.0, len_min=5, len_max=400)
+    assert np.array_equal(off, off2) and np.array_equal(w, w2)
+    lens = np.diff(off)
+    assert lens.min() >= 5 and lens.max() <= 400
+    assert abs(math.log(np.median(lens)) - math.log(150)) < 0.1
+    assert w.min() >= 0 and w.max() < c.info.vocab
+    f_req = np.bincount(w, minlength=c.info.vocab).astype(np.float64)
+    f_cor = c.word_count().astype(np.float64)
+    top = slice(0, 200)
+    r = np.corrcoef(f_req[top], f_cor[top])[0, 1]
+    assert r > 0.9, r
+    off3, _ = c.generate_requests(10, seed=10)
+    assert not np.array_equal(off3, off[:11])
+    with pytest.raises(L.LdaError):
+        c.generate_requests(3, seed=1, len_min=0)

@@ -164,3 +164,58 @@ def test_iterate_is_deterministic_across_thread_counts():
         res.append((zz, lls))
     assert np.array_equal(res[0][0], res[1][0])
     assert res[0][1] == res[1][1]
+
+
+def test_foldin_keys_and_theta_formula():
+    """Fold-in randoms: u = (x0>>8)*2^-24 with ctr = {pos, rid, sweep, 'FOLD'}; initial
+    topics (x0*K)>>32 with ctr = {pos, rid, 0xFFFFFFFF, 'FINI'}; with zero sweeps theta is
+    ((float)n_dk + alpha) / ((float)len + (float)K*alpha) of the initial topics."""
+    from oracle import lib
+    seed, rid, K = 2**33 + 9, 17, 48
+    for pos, sw in [(0, 0), (5, 3), (65534, 29)]:
+        x = philox4x32_10([pos, rid, sw, 0x464F4C44], [seed & 0xFFFFFFFF, seed >> 32])
+        assert lib().orc_foldin_uniform(seed, rid, sw, pos) == np.float32((int(x[0]) >> 8) * 2.0**-24)
+        y = philox4x32_10([pos, rid, 0xFFFFFFFF, 0x46494E49], [seed & 0xFFFFFFFF, seed >> 32])
+        assert lib().orc_foldin_init(seed, rid, pos, K) == (int(y[0]) * K) >> 32
+    c = _small_corpus(D=80, V=120, K=K, chunks=1, seed=5)
+    i = c.info
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, 50.0 / K, 0.01, nthreads=2)
+    o.rebuild(c.topics())
+    words = np.arange(37, dtype=np.int32) % i.vocab
+    z, th = o.foldin(words, rid, seed, 0)
+    assert [int(t) for t in z] == [lib().orc_foldin_init(seed, rid, p, K) for p in range(len(words))]
+    a = np.float32(o.alpha)
+    h = np.bincount(z, minlength=K).astype(np.float32)
+    assert np.array_equal(th, (h + a) / (np.float32(len(words)) + np.float32(K) * a))
+    z1, th1 = o.foldin(words, rid, seed, 4)
+    z2, th2 = o.foldin(words, rid, seed, 4)
+    assert np.array_equal(z1, z2) and np.array_equal(th1, th2)
+    with pytest.raises(ValueError):
+        o.foldin(np.array([i.vocab], dtype=np.int32), 0, seed, 1)
+
+
+def test_foldin_draw_matches_exact_conditional():
+    """Chi-square of one-sweep fold-in draws of one token (over request ids, each with its
+    own initial topics) against the summed FP64 conditionals (n_dk + alpha) * phi_wk of
+    the frozen word side."""
+    K = 16
+    c = _small_corpus(D=60, V=80, K=K, chunks=1, seed=4)
+    i = c.info
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, 50.0 / K, 0.01, nthreads=2)
+    o.rebuild(c.topics())
+    words = np.array([3, 3, 10, 41, 7, 3, 55, 10, 0, 79, 12, 3], dtype=np.int32)
+    phi = {int(w): o.phi_row(int(w)).astype(np.float64) for w in np.unique(words)}
+    n, tok = 3000, 5
+    obs = np.zeros(K, np.int64)
+    exp = np.zeros(K, np.float64)
+    for rid in range(n):
+        z0, _ = o.foldin(words, rid, 99, 0)
+        z1, _ = o.foldin(words, rid, 99, 1)
+        h = np.bincount(z0, minlength=K).astype(np.float64)
+        p = (h + o.alpha) * phi[int(words[tok])]
+        exp += p / p.sum()
+        obs[z1[tok]] += 1
+    m = exp > 5
+    chi2 = (((obs - exp) ** 2)[m] / exp[m]).sum()
+    dof = m.sum() - 1
+    assert chi2 < dof + 4.5 * np.sqrt(2 * dof) + 10, (chi2, dof)
