@@ -50,7 +50,9 @@ typedef struct {
     double len_p1, len_p2;
     int32_t len_min, len_max; /* clip */
     int32_t phi_kind;    /* 0: phi_k ~ Dir(phi_conc * 1_V);
-                            1: phi_k ~ Dir(phi_conc * V * z), z_r ∝ (r+1)^-phi_zipf_s, sum z = 1 */
+                            1: phi_k ~ Dir(phi_conc * V * z), z_r ∝ (r+1)^-phi_zipf_s, sum z = 1;
+                            2: kind 1 drawn in its Polya-urn form (phi integrated out), for
+                               gen_topics * V too large to hold explicit distributions */
     double phi_conc, phi_zipf_s;
     double theta_conc;   /* theta_d ~ Dir(theta_conc * 1_T) */
     int32_t K;           /* model topics: initial topics are uniform in [0,K) */
@@ -127,6 +129,9 @@ typedef struct {
     uint64_t seed;          /* Philox seed of the sweep randoms */
     int32_t device;         /* CUDA device ordinal */
     int64_t device_budget;  /* bytes the trainer may allocate (0: no limit) */
+    int32_t stream_mode;    /* 0: keep the corpus resident when it fits device_budget, else
+                               stream it; 1: always resident; 2: always stream */
+    int32_t num_streams;    /* streaming: CUDA streams = chunk slots on the device (0: 4) */
 } lda_train_config;
 
 /* Sweep counters accumulated since the trainer was created or lda_trainer_reset_stats. */
@@ -158,6 +163,10 @@ typedef struct {
  * WTDense.cu:27-43) and uploads it.  Fails with LDA_ERR_DEVICE_MEM when the
  * allocation would exceed cfg->device_budget or cudaMalloc fails. */
 int lda_trainer_create(const lda_corpus* c, const lda_train_config* cfg, lda_trainer** out);
+/* Whether the trainer streams its chunks (EZLDA's DataChunk/WTChunk streaming,
+ * EZLDA/mainKernel.cu:203-314), through how many streams, and the bytes it has copied
+ * host->device for chunks since creation. */
+int lda_trainer_stream_info(const lda_trainer* t, int32_t* streaming, int32_t* streams, int64_t* h2d_bytes);
 int lda_trainer_destroy(lda_trainer* t);
 /* Makes the trainer launch on an external cudaStream_t (NULL: its own stream). */
 int lda_trainer_set_stream(lda_trainer* t, void* cuda_stream);

@@ -37,6 +37,9 @@ def corpus_config(name: str, **over) -> GenConfig:
     c1: D=300,000, V=100,000, len~lognormal(5.3,0.6) in [20,2000], 256 generating
         topics, phi~Dir(0.05*V*z) with z a Zipf(1.05) base over word rank, theta~Dir(0.1),
         K=1024, dense words: top 2% by frequency, 8 chunks.
+    c2: D=1,000,000, V=1,000,000, len~Poisson(250), 1,000 generating topics with c1's
+        phi prior in its urn form, K=10,000, dense words: top 20,000, 8 chunks
+        (alpha=0.1 for this corpus).
     """
     presets = {
         "c0": dict(num_docs=2000, vocab=5000, gen_topics=32, len_kind=0, len_p1=100.0, len_p2=0.0,
@@ -51,6 +54,13 @@ def corpus_config(name: str, **over) -> GenConfig:
     # c1 at one fifth of the documents (~14M tokens): same distributions, sized for
     # profiler captures that must still exceed the 126 MB L2
     presets["c1s"] = dict(presets["c1"], num_docs=60000, vocab=60000)
+    # c2: the large-K corpus, D=1,000,000, V=1,000,000, len~Poisson(250) (~250M tokens),
+    # 1,000 generating topics with c1's Zipf base in the urn form, K=10,000, the top
+    # 20,000 words dense, 8 chunks
+    presets["c2"] = dict(num_docs=1000000, vocab=1000000, gen_topics=1000, len_kind=0, len_p1=250.0,
+                         len_p2=0.0, len_min=1, len_max=2000, phi_kind=2, phi_conc=0.05, phi_zipf_s=1.05,
+                         theta_conc=0.1, K=10000, dense_kind=2, dense_param=20000.0, num_chunks=8,
+                         corpus_seed=1002, topic_seed=42)
     if name not in presets:
         raise KeyError(f"unknown corpus preset {name!r} (have {sorted(presets)})")
     d = dict(presets[name])
@@ -180,11 +190,13 @@ class Trainer:
     """Device-resident collapsed-Gibbs sweep (EZLDA/mainKernel.cu:158-380)."""
 
     def __init__(self, corpus: Corpus, K: int, alpha: float | None = None, beta: float = 0.01,
-                 seed: int = 42, device: int = 0, device_budget: int = 0):
+                 seed: int = 42, device: int = 0, device_budget: int = 0, stream_mode: int = 0,
+                 num_streams: int = 0):
         self._lib = load()
         if alpha is None:
             alpha = 50.0 / K  # EZLDA/Argument.cuh:9
-        cfg = TrainConfig(K=K, alpha=alpha, beta=beta, seed=seed, device=device, device_budget=device_budget)
+        cfg = TrainConfig(K=K, alpha=alpha, beta=beta, seed=seed, device=device, device_budget=device_budget,
+                          stream_mode=stream_mode, num_streams=num_streams)
         h = C.c_void_p()
         check(self._lib.lda_trainer_create(corpus._h, C.byref(cfg), C.byref(h)))
         self._h = h
@@ -286,6 +298,12 @@ class Trainer:
         p, n = C.c_void_p(), C.c_int64()
         check(self._lib.lda_trainer_topics_device(self._h, C.byref(p), C.byref(n)))
         return p.value or 0, n.value
+
+    def stream_info(self) -> tuple[bool, int, int]:
+        """(streams its chunks, streams, host->device chunk bytes copied so far)."""
+        a, b, c = C.c_int32(), C.c_int32(), C.c_int64()
+        check(self._lib.lda_trainer_stream_info(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return bool(a.value), b.value, c.value
 
     @property
     def device_bytes(self) -> int:

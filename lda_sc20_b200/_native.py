@@ -45,7 +45,8 @@ class CorpusInfo(C.Structure):
 class TrainConfig(C.Structure):
     _fields_ = [
         ("K", C.c_int32), ("alpha", C.c_float), ("beta", C.c_float), ("seed", C.c_uint64),
-        ("device", C.c_int32), ("device_budget", C.c_int64),
+        ("device", C.c_int32), ("device_budget", C.c_int64), ("stream_mode", C.c_int32),
+        ("num_streams", C.c_int32),
     ]
 
 
@@ -135,6 +136,7 @@ SIGNATURES = {
     "lda_server_poll": (I32, [P, P, P, P]),
     "lda_server_status": (I32, [P, P, P, P]),
     "lda_server_get_topics": (I32, [P, U32, P, I32]),
+    "lda_trainer_stream_info": (I32, [P, P, P, P]),
     "lda_corpus_generate_requests": (I32, [P, U64, I64, F64, F64, I32, I32, P, P, I64]),
     "lda_server_set_item_tokens": (I32, [P, I32]),
     "lda_server_stats": (I32, [P, P, P]),

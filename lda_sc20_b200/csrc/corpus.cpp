@@ -223,6 +223,7 @@ int check_gen_config(const lda_gen_config* g) {
         return fail(LDA_ERR_ARG, "lda_corpus_generate: invalid configuration");
     if (g->len_kind == 0 && (g->len_p1 <= 0 || g->len_p1 > 700))
         return fail(LDA_ERR_ARG, "Poisson mean must be in (0,700]");
+    if (g->phi_kind < 0 || g->phi_kind > 2) return fail(LDA_ERR_ARG, "phi_kind must be 0, 1 or 2");
     return LDA_OK;
 }
 
@@ -233,10 +234,10 @@ int64_t draw_length(Rng& rng, int32_t kind, double p1, double p2, int32_t lo, in
     return std::max<int64_t>(lo, std::min<int64_t>(hi, L));
 }
 
-// The generating topic-word distributions phi_t ~ Dir(a), one alias table per topic.
-std::vector<Alias> draw_phi(Rng& rng, const lda_gen_config* g) {
+// The Dirichlet parameter of phi_t: a_w = phi_conc (kind 0) or phi_conc * V * z_w with z a
+// Zipf(phi_zipf_s) base over word rank (kinds 1 and 2).
+std::vector<double> phi_base(const lda_gen_config* g) {
     const int64_t V = g->vocab;
-    const int32_t T = g->gen_topics;
     std::vector<double> a(V);
     if (g->phi_kind == 0) {
         std::fill(a.begin(), a.end(), g->phi_conc);
@@ -245,24 +246,62 @@ std::vector<Alias> draw_phi(Rng& rng, const lda_gen_config* g) {
         for (int64_t r = 0; r < V; ++r) zs += std::pow((double)(r + 1), -g->phi_zipf_s);
         for (int64_t r = 0; r < V; ++r) a[r] = g->phi_conc * (double)V * std::pow((double)(r + 1), -g->phi_zipf_s) / zs;
     }
-    std::vector<Alias> phi(T);
-    std::vector<double> lg(V), p(V);
-    for (int32_t t = 0; t < T; ++t) {
-        double mx = -INFINITY;
-        for (int64_t v = 0; v < V; ++v) { lg[v] = rng.log_gamma_draw(a[v]); mx = std::max(mx, lg[v]); }
-        double s = 0.0;
-        for (int64_t v = 0; v < V; ++v) { p[v] = std::exp(lg[v] - mx); s += p[v]; }
-        for (int64_t v = 0; v < V; ++v) p[v] /= s;
-        phi[t].build(p);
-    }
-    return phi;
+    return a;
 }
 
+// Word draws of the generating topics.  Kinds 0 and 1 draw phi_t ~ Dir(a) explicitly (one
+// alias table per topic, T*V gamma draws).  Kind 2 draws the same process in its Polya-urn
+// form, for T*V too large to materialise: topic t's n-th word is a copy of one of its n
+// earlier words with probability n/(n+A), else a fresh draw from the base a/A (A = sum a),
+// which is the predictive of words drawn i.i.d. from phi_t ~ Dir(a) with phi_t integrated out.
+struct TopicWords {
+    std::vector<Alias> phi;                  // kinds 0, 1
+    Alias base;                              // kind 2
+    double A = 0.0;
+    std::vector<std::vector<int32_t>> drawn; // kind 2: words drawn so far per topic
+    bool urn = false;
+
+    void init(Rng& rng, const lda_gen_config* g) {
+        const int64_t V = g->vocab;
+        const int32_t T = g->gen_topics;
+        std::vector<double> a = phi_base(g);
+        if (g->phi_kind == 2) {
+            urn = true;
+            A = 0.0;
+            for (double x : a) A += x;
+            std::vector<double> p(V);
+            for (int64_t v = 0; v < V; ++v) p[v] = a[v] / A;
+            base.build(p);
+            drawn.assign(T, {});
+            return;
+        }
+        phi.resize(T);
+        std::vector<double> lg(V), p(V);
+        for (int32_t t = 0; t < T; ++t) {
+            double mx = -INFINITY;
+            for (int64_t v = 0; v < V; ++v) { lg[v] = rng.log_gamma_draw(a[v]); mx = std::max(mx, lg[v]); }
+            double s = 0.0;
+            for (int64_t v = 0; v < V; ++v) { p[v] = std::exp(lg[v] - mx); s += p[v]; }
+            for (int64_t v = 0; v < V; ++v) p[v] /= s;
+            phi[t].build(p);
+        }
+    }
+
+    int32_t draw(Rng& rng, int32_t t) {
+        if (!urn) return phi[t].draw(rng.u01());
+        std::vector<int32_t>& L = drawn[t];
+        const double n = (double)L.size();
+        const double x = rng.u01() * (n + A);
+        const int32_t w = x < n ? L[(size_t)x] : base.draw(rng.u01());
+        L.push_back(w);
+        return w;
+    }
+};
+
 // Tokens of one document of length L: topics by the Polya urn of theta ~ Dir(theta_conc),
-// words from phi.
-void draw_doc(Rng& rng, const std::vector<Alias>& phi, double theta_conc, int64_t L, std::vector<int32_t>& tt,
+// words from the topics' word draws.
+void draw_doc(Rng& rng, TopicWords& tw, int32_t T, double theta_conc, int64_t L, std::vector<int32_t>& tt,
               int32_t* out) {
-    const int32_t T = (int32_t)phi.size();
     const double Ta = (double)T * theta_conc;
     tt.resize(L);
     for (int64_t i = 0; i < L; ++i) {
@@ -271,7 +310,7 @@ void draw_doc(Rng& rng, const std::vector<Alias>& phi, double theta_conc, int64_
         if (x < (double)i) t = tt[(int64_t)x];
         else t = std::min<int32_t>(T - 1, (int32_t)((x - (double)i) / theta_conc));
         tt[i] = t;
-        out[i] = phi[t].draw(rng.u01());
+        out[i] = tw.draw(rng, t);
     }
 }
 
@@ -291,12 +330,13 @@ extern "C" int lda_corpus_generate(const lda_gen_config* g, lda_corpus** out) {
             doc_off[d + 1] = doc_off[d] + draw_length(rng, g->len_kind, g->len_p1, g->len_p2, g->len_min, g->len_max);
         const int64_t N = doc_off[D];
         // 2. topic-word distributions
-        std::vector<Alias> phi = draw_phi(rng, g);
+        TopicWords tw;
+        tw.init(rng, g);
         // 3. tokens
         std::vector<int32_t> raw(N), tt;
-        for (int64_t d = 0; d < D; ++d) draw_doc(rng, phi, g->theta_conc, doc_off[d + 1] - doc_off[d], tt, raw.data() + doc_off[d]);
-        phi.clear();
-        phi.shrink_to_fit();
+        for (int64_t d = 0; d < D; ++d)
+            draw_doc(rng, tw, g->gen_topics, g->theta_conc, doc_off[d + 1] - doc_off[d], tt, raw.data() + doc_off[d]);
+        tw = TopicWords();
         // 4. frequency ranks, dense split, layout
         std::vector<int64_t> cnt(V, 0);
         for (int64_t j = 0; j < N; ++j) cnt[raw[j]]++;
@@ -335,15 +375,18 @@ extern "C" int lda_corpus_generate_requests(const lda_corpus* c, uint64_t reques
         if (cap < doc_off[n]) return fail(LDA_ERR_ARG, "words holds %lld entries, %lld needed", (long long)cap, (long long)doc_off[n]);
         // the corpus' generating phi: replay its stream through the doc lengths
         const lda_gen_config* g = &c->gen;
+        if (g->phi_kind == 2)
+            return fail(LDA_ERR_STATE, "requests need an explicit phi (phi_kind 0 or 1); this corpus used the urn form");
         Rng rng(g->corpus_seed);
         for (int64_t d = 0; d < g->num_docs; ++d) draw_length(rng, g->len_kind, g->len_p1, g->len_p2, g->len_min, g->len_max);
-        const std::vector<Alias> phi = draw_phi(rng, g);
+        TopicWords tw;
+        tw.init(rng, g);
         Rng drng(request_seed);
         std::vector<int32_t> tt;
         for (int64_t i = 0; i < n; ++i) {
             int32_t* w = words + doc_off[i];
             const int64_t L = doc_off[i + 1] - doc_off[i];
-            draw_doc(drng, phi, g->theta_conc, L, tt, w);
+            draw_doc(drng, tw, g->gen_topics, g->theta_conc, L, tt, w);
             for (int64_t j = 0; j < L; ++j) w[j] = c->rank_of[w[j]];
         }
         return LDA_OK;

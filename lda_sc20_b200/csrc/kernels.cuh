@@ -169,6 +169,10 @@ struct DtArgs {
     uint32_t* dt_ent;
     uint32_t* meta;             // [N] word-sorted: (n_d,2nd << 16) | n_d,max
     int* err;
+    // dtok_pos / dtok_word / meta hold tokens [tok_base, ...) and dt_ent the doc-row
+    // entries [dt_base, ...): 0 when the whole corpus is resident, the chunk's first token
+    // and first doc-row entry when the chunk is streamed into a slot buffer
+    uint32_t tok_base, dt_base;
 };
 
 __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
@@ -181,7 +185,7 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
         const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
         for (uint32_t base = 0; base < n; base += 32) {
             bool valid = base + lane < n;
-            uint32_t k = valid ? (uint32_t)__ldg(a.z + __ldg(a.dtok_pos + b + base + lane)) : 0xffffffffu;
+            uint32_t k = valid ? (uint32_t)__ldg(a.z + __ldg(a.dtok_pos + (b - a.tok_base) + base + lane)) : 0xffffffffu;
             if (valid && k >= (uint32_t)a.K) {
                 atomicOr(a.err, 1);
                 valid = false;
@@ -192,14 +196,14 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
         }
         __syncwarp();
         for (uint32_t i = lane; i < n; i += 32) {
-            const uint32_t pos = __ldg(a.dtok_pos + b + i);
-            const uint32_t t2 = __ldg(a.st_top2 + __ldg(a.dtok_word + b + i));
+            const uint32_t pos = __ldg(a.dtok_pos + (b - a.tok_base) + i);
+            const uint32_t t2 = __ldg(a.st_top2 + __ldg(a.dtok_word + (b - a.tok_base) + i));
             const uint32_t k1 = t2 & 0xffffu, k2 = t2 >> 16;
             const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
-            a.meta[pos] = (c2 << 16) | c1;
+            a.meta[pos - a.tok_base] = (c2 << 16) | c1;
         }
         __syncwarp();
-        uint32_t* out = a.dt_ent + __ldg(a.dt_off + d);
+        uint32_t* out = a.dt_ent + (__ldg(a.dt_off + d) - a.dt_base);
         uint32_t nnz = 0;
         for (int kb = 0; kb < a.K; kb += 32) {
             const int k = kb + lane;
@@ -258,6 +262,9 @@ struct SampleArgs {
     const uint32_t* dt_ent;
     // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles, rows, row entries
     unsigned long long* ctr;
+    // tok_doc / meta hold tokens [tok_base, ...) and dt_ent the doc-row entries
+    // [dt_base, ...) (non-zero when the chunk is streamed into a slot buffer)
+    uint32_t tok_base, dt_base;
 };
 
 // Sweep counters live in shared memory (one row per warp, written by lane 0) so they
@@ -314,11 +321,11 @@ __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleA
             float u = 0.0f, pmax = 0.0f;
             bool ea = false;
             if (valid) {
-                d = __ldg(a.tok_doc + tok);
-                const uint32_t m = __ldg(a.meta + tok);
+                d = __ldg(a.tok_doc + (tok - a.tok_base));
+                const uint32_t m = __ldg(a.meta + (tok - a.tok_base));
                 nd = __ldg(a.doc_len + d);
                 my_nnz = __ldg(a.dt_nnz + d);
-                my_off = __ldg(a.dt_off + d);
+                my_off = __ldg(a.dt_off + d) - a.dt_base;
                 const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
                 u = token_uniform(a.seed_lo, a.seed_hi, a.iter, tok);
                 pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);

@@ -80,11 +80,37 @@ struct lda_trainer {
     std::vector<bool> chunk_sampled_ll;
     int chunk_first = 0, chunk_last = 0;  // sampled chunk range of lda_trainer_iterate
 
+    // streaming: the per-token arrays of the doc-topic rebuild and the sampler (doc of each
+    // token, doc-order -> word-sorted map and word, per-token metadata) and the doc rows
+    // live in one slot buffer per stream; the static ones are copied in from pinned host
+    // memory for every chunk of every sweep
+    struct Slot {
+        uint32_t *tok_doc = nullptr, *dtok_pos = nullptr, *dtok_word = nullptr, *meta = nullptr, *dt_ent = nullptr;
+        int chunk = -1;  // chunk whose static arrays the slot holds (stage entry points)
+    };
+    bool streaming = false;
+    std::vector<cudaStream_t> sstreams;
+    std::vector<Slot> slots;
+    std::vector<cudaEvent_t> ev_slot;
+    cudaEvent_t ev_ready = nullptr;
+    uint32_t *h_tok_doc = nullptr, *h_dtok_pos = nullptr, *h_dtok_word = nullptr;  // pinned [N]
+    std::vector<int64_t> chunk_dt;  // [C+1] first doc-row entry of each chunk
+    int64_t max_chunk_tok = 0, max_chunk_dt = 0, h2d_bytes = 0;
+
     int64_t range_tokens() const { return chunk_tok[chunk_last] - chunk_tok[chunk_first]; }
 
     ~lda_trainer() {
         if (device >= 0) cudaSetDevice(device);
         if (stream) cudaStreamSynchronize(stream);
+        for (cudaStream_t q : sstreams) {
+            cudaStreamSynchronize(q);
+            cudaStreamDestroy(q);
+        }
+        for (cudaEvent_t e : ev_slot) cudaEventDestroy(e);
+        if (ev_ready) cudaEventDestroy(ev_ready);
+        cudaFreeHost(h_tok_doc);
+        cudaFreeHost(h_dtok_pos);
+        cudaFreeHost(h_dtok_word);
         for (void* p : allocs) cudaFree(p);
         if (ll_host) cudaFreeHost(ll_host);
         for (auto& e : pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -249,11 +275,63 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     std::stable_sort(wt.begin(), wt.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
     T.n_wtiles = (int)wt.size();
 
-    // ---- device allocation (Document/DTChunk/WTAll/WTD::GPUMemAllocate)
+    // ---- resident or streamed chunks (EZLDA streams every chunk through fixed buffers,
+    // EZLDA/mainKernel.cu:203-314; here the corpus stays resident when it fits the budget)
+    if (cfg->stream_mode < 0 || cfg->stream_mode > 2) return fail(LDA_ERR_ARG, "stream_mode %d", cfg->stream_mode);
+    if (cfg->num_streams < 0 || cfg->num_streams > 64) return fail(LDA_ERR_ARG, "num_streams %d", cfg->num_streams);
+    T.chunk_dt.assign(T.C + 1, 0);
+    for (int ch = 0; ch < T.C; ++ch) {
+        const int64_t d0 = T.chunk_doc[ch], d1 = T.chunk_doc[ch + 1];
+        T.chunk_dt[ch] = d0 < D ? hdt_off[d0] : T.dt_cap;
+        T.chunk_dt[ch + 1] = d1 < D ? hdt_off[d1] : T.dt_cap;
+        T.max_chunk_tok = std::max(T.max_chunk_tok, T.chunk_tok[ch + 1] - T.chunk_tok[ch]);
+    }
+    for (int ch = 0; ch < T.C; ++ch) T.max_chunk_dt = std::max(T.max_chunk_dt, T.chunk_dt[ch + 1] - T.chunk_dt[ch]);
+    {
+        // the exact bytes of the resident layout (the allocations below, in resident mode)
+        auto nb = [](int64_t n, int64_t size) { return std::max<int64_t>(n, 1) * size; };
+        const int64_t ns = (int64_t)st.size(), nw = (int64_t)wt.size();
+        const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
+                                 nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
+                                 nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
+                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + T.C, 4) + nb(kCounters, 8) +
+                                 nb(1, 4);
+        T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
+    }
     int rc;
 #define ALLOC(p, n) if ((rc = T.alloc(&(p), (n))) != LDA_OK) return rc
-    ALLOC(T.tok_doc, N); ALLOC(T.meta, N); ALLOC(T.dtok_pos, N); ALLOC(T.dtok_word, N); ALLOC(T.z, N);
-    ALLOC(T.doc_off, D + 1); ALLOC(T.doc_len, D); ALLOC(T.dt_off, D); ALLOC(T.dt_nnz, D); ALLOC(T.dt_ent, T.dt_cap);
+    if (!T.streaming) {
+        ALLOC(T.tok_doc, N); ALLOC(T.meta, N); ALLOC(T.dtok_pos, N); ALLOC(T.dtok_word, N); ALLOC(T.dt_ent, T.dt_cap);
+    } else {
+        const int ns = cfg->num_streams > 0 ? cfg->num_streams : 4;
+        T.slots.resize(ns);
+        for (auto& sl : T.slots) {
+            ALLOC(sl.tok_doc, T.max_chunk_tok); ALLOC(sl.dtok_pos, T.max_chunk_tok); ALLOC(sl.dtok_word, T.max_chunk_tok);
+            ALLOC(sl.meta, T.max_chunk_tok); ALLOC(sl.dt_ent, T.max_chunk_dt);
+        }
+        T.sstreams.resize(ns, nullptr);
+        T.ev_slot.resize(ns, nullptr);
+        for (int i = 0; i < ns; ++i) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&T.sstreams[i], cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&T.ev_slot[i], cudaEventDisableTiming));
+        }
+        CUDA_TRY(cudaEventCreateWithFlags(&T.ev_ready, cudaEventDisableTiming));
+        const size_t nb = sizeof(uint32_t) * (size_t)std::max<int64_t>(N, 1);
+        cudaError_t e = cudaMallocHost(&T.h_tok_doc, nb);
+        if (e == cudaSuccess) e = cudaMallocHost(&T.h_dtok_pos, nb);
+        if (e == cudaSuccess) e = cudaMallocHost(&T.h_dtok_word, nb);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(LDA_ERR_NOMEM, "pinned host staging of %zu bytes failed: %s", 3 * nb, cudaGetErrorString(e));
+        }
+        for (int64_t i = 0; i < N; ++i) {
+            T.h_tok_doc[i] = (uint32_t)c->tok_doc[i];
+            T.h_dtok_pos[i] = (uint32_t)c->dtok_pos[i];
+            T.h_dtok_word[i] = (uint32_t)c->dtok_word[i];
+        }
+    }
+    ALLOC(T.z, N);
+    ALLOC(T.doc_off, D + 1); ALLOC(T.doc_len, D); ALLOC(T.dt_off, D); ALLOC(T.dt_nnz, D);
     ALLOC(T.dwt, (int64_t)T.Vd * T.K); ALLOC(T.swt_off, std::max<int64_t>(Vs, 1)); ALLOC(T.swt_nnz, std::max<int64_t>(Vs, 1));
     ALLOC(T.swt_ent, T.swt_cap);
     ALLOC(T.n_k, T.K); ALLOC(T.st_top2, V); ALLOC(T.st_k3, V); ALLOC(T.st_phi, V); ALLOC(T.st_ql, V * 32);
@@ -270,9 +348,12 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         CUDA_TRY(cudaMemcpy(dst, h32.data(), sizeof(uint32_t) * (size_t)n, cudaMemcpyHostToDevice));
         return LDA_OK;
     };
-    if ((rc = up32(T.tok_doc, N, [&](int64_t i) { return c->tok_doc[i]; }))) return rc;
-    if ((rc = up32(T.dtok_pos, N, [&](int64_t i) { return c->dtok_pos[i]; }))) return rc;
-    if ((rc = up32(T.dtok_word, N, [&](int64_t i) { return c->dtok_word[i]; }))) return rc;
+    if (!T.streaming) {
+        if ((rc = up32(T.tok_doc, N, [&](int64_t i) { return c->tok_doc[i]; }))) return rc;
+        if ((rc = up32(T.dtok_pos, N, [&](int64_t i) { return c->dtok_pos[i]; }))) return rc;
+        if ((rc = up32(T.dtok_word, N, [&](int64_t i) { return c->dtok_word[i]; }))) return rc;
+        CUDA_TRY(cudaMemset(T.meta, 0, sizeof(uint32_t) * (size_t)N));
+    }
     if ((rc = up32(T.doc_off, D + 1, [&](int64_t i) { return c->doc_off[i]; }))) return rc;
     if ((rc = up32(T.seg_off, (int64_t)T.C * V, [&](int64_t i) { return c->seg_off[i]; }))) return rc;
     if ((rc = up32(T.seg_cnt, (int64_t)T.C * V, [&](int64_t i) { return c->seg_cnt[i]; }))) return rc;
@@ -282,7 +363,6 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     if (Vs > 0) CUDA_TRY(cudaMemcpy(T.swt_off, hswt_off.data(), sizeof(uint32_t) * (size_t)Vs, cudaMemcpyHostToDevice));
     CUDA_TRY(cudaMemset(T.swt_nnz, 0, sizeof(uint32_t) * (size_t)std::max<int64_t>(Vs, 1)));
     CUDA_TRY(cudaMemset(T.dt_nnz, 0, sizeof(uint32_t) * (size_t)D));
-    CUDA_TRY(cudaMemset(T.meta, 0, sizeof(uint32_t) * (size_t)N));
     // stats start valid (topic 0) so a stage called out of order reads in-range topics
     CUDA_TRY(cudaMemset(T.st_top2, 0, sizeof(uint32_t) * (size_t)V));
     CUDA_TRY(cudaMemset(T.st_k3, 0, sizeof(uint32_t) * (size_t)V));
@@ -351,6 +431,15 @@ extern "C" int lda_trainer_topics_device(lda_trainer* t, void** ptr, int64_t* co
     return LDA_OK;
 }
 
+extern "C" int lda_trainer_stream_info(const lda_trainer* t, int32_t* streaming, int32_t* streams,
+                                       int64_t* h2d_bytes) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (streaming) *streaming = t->streaming ? 1 : 0;
+    if (streams) *streams = (int32_t)t->sstreams.size();
+    if (h2d_bytes) *h2d_bytes = t->h2d_bytes;
+    return LDA_OK;
+}
+
 extern "C" int lda_trainer_device_bytes(const lda_trainer* t, int64_t* b) {
     if (!t || !b) return fail(LDA_ERR_ARG, "null argument");
     *b = t->bytes;
@@ -393,32 +482,66 @@ extern "C" int lda_max_topic(lda_trainer* t) {
     return LDA_OK;
 }
 
-extern "C" int lda_update_dt(lda_trainer* t, int32_t chunk) {
-    if (!t) return fail(LDA_ERR_ARG, "null trainer");
-    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
-    CUDA_TRY(cudaSetDevice(t->device));
-    t->begin_stage(2);
-    dev::DtArgs a;
-    a.d_begin = (uint32_t)t->chunk_doc[chunk]; a.d_end = (uint32_t)t->chunk_doc[chunk + 1]; a.K = t->K;
-    a.doc_off = t->doc_off; a.dtok_pos = t->dtok_pos; a.dtok_word = t->dtok_word; a.z = t->z;
-    a.st_top2 = t->st_top2; a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = t->dt_ent; a.meta = t->meta;
-    a.err = t->err;
-    const int64_t nd = a.d_end - a.d_begin;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps - 1) / t->warps));
-    dev::k_dt_build<<<grid, 32 * t->warps, t->smem_dt, t->stream>>>(a);
-    CUDA_TRY(cudaGetLastError());
-    t->end_stage();
+// Buffers holding a chunk's per-token arrays and doc rows: the resident arrays, or the
+// chunk's slot when streaming.
+struct ChunkBufs {
+    const uint32_t *tok_doc, *dtok_pos, *dtok_word;
+    uint32_t *meta, *dt_ent;
+    uint32_t tok_base, dt_base;
+};
+
+static ChunkBufs chunk_bufs(const lda_trainer* t, int chunk, int slot) {
+    ChunkBufs b;
+    if (!t->streaming) {
+        b.tok_doc = t->tok_doc; b.dtok_pos = t->dtok_pos; b.dtok_word = t->dtok_word;
+        b.meta = t->meta; b.dt_ent = t->dt_ent;
+        b.tok_base = b.dt_base = 0;
+    } else {
+        const auto& sl = t->slots[slot];
+        b.tok_doc = sl.tok_doc; b.dtok_pos = sl.dtok_pos; b.dtok_word = sl.dtok_word;
+        b.meta = sl.meta; b.dt_ent = sl.dt_ent;
+        b.tok_base = (uint32_t)t->chunk_tok[chunk];
+        b.dt_base = (uint32_t)t->chunk_dt[chunk];
+    }
+    return b;
+}
+
+// Streaming: copies a chunk's static per-token arrays into its slot on stream `q`.
+static int load_chunk(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
+    auto& sl = t->slots[slot];
+    const int64_t t0 = t->chunk_tok[chunk], n = t->chunk_tok[chunk + 1] - t0;
+    if (n > 0) {
+        const size_t nb = sizeof(uint32_t) * (size_t)n;
+        CUDA_TRY(cudaMemcpyAsync(sl.tok_doc, t->h_tok_doc + t0, nb, cudaMemcpyHostToDevice, q));
+        CUDA_TRY(cudaMemcpyAsync(sl.dtok_pos, t->h_dtok_pos + t0, nb, cudaMemcpyHostToDevice, q));
+        CUDA_TRY(cudaMemcpyAsync(sl.dtok_word, t->h_dtok_word + t0, nb, cudaMemcpyHostToDevice, q));
+        t->h2d_bytes += 3 * (int64_t)nb;
+    }
+    sl.chunk = chunk;
     return LDA_OK;
 }
 
-extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) {
-    if (!t) return fail(LDA_ERR_ARG, "null trainer");
-    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
-    CUDA_TRY(cudaSetDevice(t->device));
-    t->begin_stage(3);
+static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
+    const ChunkBufs b = chunk_bufs(t, chunk, slot);
+    dev::DtArgs a;
+    a.d_begin = (uint32_t)t->chunk_doc[chunk]; a.d_end = (uint32_t)t->chunk_doc[chunk + 1]; a.K = t->K;
+    a.doc_off = t->doc_off; a.dtok_pos = b.dtok_pos; a.dtok_word = b.dtok_word; a.z = t->z;
+    a.st_top2 = t->st_top2; a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.meta = b.meta;
+    a.err = t->err;
+    a.tok_base = b.tok_base;
+    a.dt_base = b.dt_base;
+    const int64_t nd = a.d_end - a.d_begin;
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps - 1) / t->warps));
+    dev::k_dt_build<<<grid, 32 * t->warps, t->smem_dt, q>>>(a);
+    CUDA_TRY(cudaGetLastError());
+    return LDA_OK;
+}
+
+static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaStream_t q) {
+    const ChunkBufs b = chunk_bufs(t, chunk, slot);
     const int base = t->s_tile_base[chunk], n = t->s_tile_base[chunk + 1] - base;
     unsigned* ctr = t->tile_ctr + 1 + chunk;
-    CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned), t->stream));
+    CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned), q));
     dev::SampleArgs a;
     a.tiles = t->s_tiles + base; a.ntiles = n; a.tile_counter = ctr; a.tile_ll = t->tile_ll + base;
     a.K = t->K; a.Vd = t->Vd; a.ll_mode = ll_mode ? 1 : 0;
@@ -427,16 +550,48 @@ extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) 
     a.seed_lo = (uint32_t)t->seed; a.seed_hi = (uint32_t)(t->seed >> 32); a.iter = t->iter;
     a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
     a.st_top2 = t->st_top2; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
-    a.tok_doc = t->tok_doc; a.meta = t->meta; a.z = t->z; a.doc_len = t->doc_len;
-    a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = t->dt_ent; a.ctr = t->ctr;
+    a.tok_doc = b.tok_doc; a.meta = b.meta; a.z = t->z; a.doc_len = t->doc_len;
+    a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.ctr = t->ctr;
+    a.tok_base = b.tok_base;
+    a.dt_base = b.dt_base;
     if (n > 0) {
         const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
-        if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
-        else dev::k_sample_t<false><<<grid, 32 * t->warps, t->smem_sample, t->stream>>>(a);
+        if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * t->warps, t->smem_sample, q>>>(a);
+        else dev::k_sample_t<false><<<grid, 32 * t->warps, t->smem_sample, q>>>(a);
         CUDA_TRY(cudaGetLastError());
     }
-    t->end_stage();
     t->chunk_sampled_ll[chunk] = ll_mode != 0;
+    return LDA_OK;
+}
+
+extern "C" int lda_update_dt(lda_trainer* t, int32_t chunk) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
+    CUDA_TRY(cudaSetDevice(t->device));
+    int rc;
+    const int slot = t->streaming ? chunk % (int)t->slots.size() : 0;
+    if (t->streaming) {
+        t->begin_stage(5);
+        if ((rc = load_chunk(t, chunk, slot, t->stream))) return rc;
+        t->end_stage();
+    }
+    t->begin_stage(2);
+    if ((rc = dt_launch(t, chunk, slot, t->stream))) return rc;
+    t->end_stage();
+    return LDA_OK;
+}
+
+extern "C" int lda_sample_chunk(lda_trainer* t, int32_t chunk, int32_t ll_mode) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (chunk < 0 || chunk >= t->C) return fail(LDA_ERR_ARG, "chunk %d of %d", chunk, t->C);
+    const int slot = t->streaming ? chunk % (int)t->slots.size() : 0;
+    if (t->streaming && t->slots[slot].chunk != chunk)
+        return fail(LDA_ERR_STATE, "chunk %d is not loaded (run lda_update_dt for it first)", chunk);
+    CUDA_TRY(cudaSetDevice(t->device));
+    t->begin_stage(3);
+    int rc = sample_launch(t, chunk, slot, ll_mode, t->stream);
+    if (rc) return rc;
+    t->end_stage();
     return LDA_OK;
 }
 
@@ -493,9 +648,32 @@ static int sweep_async(lda_trainer* t, int ll_mode) {
     int rc;
     if ((rc = lda_update_wt(t))) return rc;
     if ((rc = lda_max_topic(t))) return rc;
-    for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
-        if ((rc = lda_update_dt(t, ch))) return rc;
-        if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
+    if (!t->streaming) {
+        for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
+            if ((rc = lda_update_dt(t, ch))) return rc;
+            if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
+        }
+    } else {
+        // chunk i of the range goes to slot / stream i mod S: its copy overlaps the
+        // rebuild and sampling of the chunks on the other streams; a slot is reused in
+        // stream order.  Chunks are independent within a sweep (each rebuilds its own doc
+        // rows from its own topics and writes only its own topics).
+        const int S = (int)t->slots.size();
+        t->begin_stage(3);
+        CUDA_TRY(cudaEventRecord(t->ev_ready, t->stream));
+        for (int i = 0; i < S; ++i) CUDA_TRY(cudaStreamWaitEvent(t->sstreams[i], t->ev_ready, 0));
+        for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
+            const int slot = (ch - t->chunk_first) % S;
+            cudaStream_t q = t->sstreams[slot];
+            if ((rc = load_chunk(t, ch, slot, q))) return rc;
+            if ((rc = dt_launch(t, ch, slot, q))) return rc;
+            if ((rc = sample_launch(t, ch, slot, ll_mode, q))) return rc;
+        }
+        for (int i = 0; i < S; ++i) {
+            CUDA_TRY(cudaEventRecord(t->ev_slot[i], t->sstreams[i]));
+            CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_slot[i], 0));
+        }
+        t->end_stage();
     }
     if (ll_mode && (rc = perplexity_async(t))) return rc;
     t->iter++;
@@ -741,6 +919,7 @@ extern "C" int lda_get_word_stats(lda_trainer* t, uint32_t* top2, uint32_t* k3, 
 }
 
 extern "C" int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent, int64_t cap) {
+    if (t && t->streaming) return fail(LDA_ERR_STATE, "doc rows are not kept when the corpus is streamed");
     if (!t || !off) return fail(LDA_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(t->device));
     CUDA_TRY(cudaStreamSynchronize(t->stream));
@@ -762,6 +941,7 @@ extern "C" int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent,
 }
 
 extern "C" int lda_get_token_meta(lda_trainer* t, uint32_t* meta) {
+    if (t && t->streaming) return fail(LDA_ERR_STATE, "token metadata is not kept when the corpus is streamed");
     if (!t || !meta) return fail(LDA_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(t->device));
     CUDA_TRY(cudaStreamSynchronize(t->stream));
@@ -859,6 +1039,8 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.tok_doc = io->tok_doc; a.meta = io->meta; a.z = io->topics; a.doc_len = io->doc_len;
     a.dt_off = io->dt_off; a.dt_nnz = io->dt_nnz; a.dt_ent = io->dt_ent;
     a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
+    a.tok_base = 0;
+    a.dt_base = 0;
     if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * warps, smem, st>>>(a);
     else dev::k_sample_t<false><<<grid, 32 * warps, smem, st>>>(a);
     CUDA_TRY(cudaGetLastError());

@@ -173,3 +173,19 @@ def test_generate_requests_follow_the_corpus_process():
     assert not np.array_equal(off3, off[:11])
     with pytest.raises(L.LdaError):
         c.generate_requests(3, seed=1, len_min=0)
+
+
+def test_urn_form_matches_explicit_dirichlet():
+    """phi_kind 2 (Polya urn, phi integrated out) and phi_kind 1 (explicit Dirichlet draws)
+    are the same generative process: their rank-frequency curves agree."""
+    covs = {}
+    for kind in (1, 2):
+        cov = []
+        for seed in (11, 12, 13):
+            c = L.Corpus.generate(L.corpus_config("c0", num_docs=1500, vocab=4000, gen_topics=16, phi_kind=kind,
+                                                  phi_conc=0.05, phi_zipf_s=1.05, corpus_seed=seed))
+            wc = np.sort(c.word_count())[::-1].astype(np.float64)
+            tot = wc.sum()
+            cov.append([wc[:10].sum() / tot, wc[:100].sum() / tot, wc[:1000].sum() / tot, (wc > 0).mean()])
+        covs[kind] = np.mean(cov, axis=0)
+    assert np.allclose(covs[1], covs[2], rtol=0.08, atol=0.01), covs

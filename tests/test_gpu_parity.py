@@ -96,7 +96,7 @@ def test_fifty_sweeps_bit_exact_c0():
     assert lls[-1] > lls[0]  # the chain is mixing toward higher likelihood
 
 
-@pytest.mark.parametrize("K", [4, 16, 100, 1024])
+@pytest.mark.parametrize("K", [4, 16, 100, 1024, 4096, 10000])
 def test_k_variants(K):
     c = L.Corpus.generate(L.corpus_config("c0", num_docs=500, vocab=800, K=K, num_chunks=2))
     tr, o = _setup(c, K)
@@ -235,3 +235,52 @@ def test_config1_full_size_properties():
     tr2.iterate(1, ll=True)
     assert np.array_equal(tr2.topics(), z1)
     assert tr2.loglik()[0] == ll
+
+
+@pytest.mark.parametrize("streams", [1, 2, 3])
+def test_streamed_chunks_equal_resident(streams):
+    """Chunks streamed through `streams` slot buffers (EZLDA/mainKernel.cu:203-314) give the
+    same topics, LL and counters as the resident corpus, sweep after sweep."""
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=5, dense_kind=1, dense_param=0.05))
+    K = 64
+    res = L.Trainer(c, K=K, seed=42, stream_mode=1)
+    stm = L.Trainer(c, K=K, seed=42, stream_mode=2, num_streams=streams)
+    assert res.stream_info()[0] is False
+    on, ns, _ = stm.stream_info()
+    assert on and ns == streams
+    assert stm.device_bytes < res.device_bytes
+    for it in range(6):
+        ll_r = res.iterate(1, ll=(it % 2 == 0))
+        ll_s = stm.iterate(1, ll=(it % 2 == 0))
+        assert np.array_equal(res.topics(), stm.topics()), f"sweep {it}"
+        assert ll_r == ll_s
+    a, b = res.counters(), stm.counters()
+    assert (a.tokens, a.early_accept, a.branch_q) == (b.tokens, b.early_accept, b.branch_q)
+    per_sweep = 12 * c.info.num_tokens
+    assert stm.stream_info()[2] == 6 * per_sweep
+
+
+def test_streaming_by_budget_and_stage_api():
+    """A budget below the resident layout switches to streaming; the stage entry points
+    load a chunk in lda_update_dt and refuse to sample a chunk that is not loaded."""
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=4))
+    K = 64
+    res = L.Trainer(c, K=K, seed=42)
+    full = res.device_bytes
+    stm = L.Trainer(c, K=K, seed=42, device_budget=full - 1, num_streams=2)
+    assert stm.stream_info()[0]
+    assert stm.device_bytes <= full - 1
+    o = Oracle(c.tok_word(), c.tok_doc(), c.info.vocab, c.info.num_docs, K, stm.alpha, stm.beta)
+    z = c.topics()
+    o.iterate(z, 42, 0)
+    stm.update_wt()
+    stm.max_topic()
+    with pytest.raises(L.LdaError):
+        stm.sample_chunk(1)
+    for ch in range(c.info.num_chunks):
+        stm.update_dt(ch)
+        stm.sample_chunk(ch)
+    stm.end_sweep()
+    assert np.array_equal(stm.topics(), z)
+    with pytest.raises(L.LdaError):
+        stm.doc_rows()
