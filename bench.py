@@ -33,9 +33,20 @@ sys.path.insert(0, ROOT)
 
 METRIC = "gibbs_tokens_per_s_per_iter"
 UNIT = "tokens/s"
-WORKLOAD = ("lognormal K=1024 corpus: D=300000 V=100000 len~lognormal(5.3,0.6) in [20,2000] "
-            "(~71.9M tokens), 256 generating topics, Zipf(1.05) phi base, alpha=50/K, beta=0.01, "
-            "top-2% dense words, 8 chunks; sweeps 0..K-1 from random initial topics")
+WORKLOADS = {
+    "c1": ("lognormal K=1024 corpus: D=300000 V=100000 len~lognormal(5.3,0.6) in [20,2000] "
+           "(~71.9M tokens), 256 generating topics, Zipf(1.05) phi base, alpha=50/K, beta=0.01, "
+           "top-2% dense words, 8 chunks; sweeps 0..K-1 from random initial topics"),
+    "c2": ("large-K corpus: D=1000000 V=1000000 len~Poisson(250) (~250M tokens), 1000 generating "
+           "topics, Zipf(1.05) phi base (urn form), K=10000, alpha=0.1, beta=0.01, top-20000 dense "
+           "words, 8 chunks; sweeps 0..K-1 from random initial topics"),
+}
+WORKLOAD = WORKLOADS["c1"]
+ALPHA = {"c2": 0.1}  # other presets: 50/K
+
+
+def workload(preset: str) -> str:
+    return WORKLOADS.get(preset, f"corpus preset {preset}")
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -52,6 +63,15 @@ def parse_args():
     p.add_argument("--chunks", type=int, default=0, help="override the preset's chunk count")
     p.add_argument("--sharded", action="store_true",
                    help="use the document-sharded path even on one GPU (it is the default for N>1)")
+    p.add_argument("--stream", action="store_true",
+                   help="stream the chunks through 4 CUDA streams (EZLDA's chunk streaming) instead of "
+                        "keeping the corpus resident")
+    p.add_argument("--budget-gb", type=float, default=0.0, help="device budget of the trainer (0: none)")
+    p.add_argument("--batch", action="store_true",
+                   help="batched multi-model benchmark: 512 small corpora in one graph-captured batch "
+                        "against the same models trained one after another")
+    p.add_argument("--batch-models", type=int, default=512)
+    p.add_argument("--batch-sweeps", type=int, default=100)
     p.add_argument("--serve", action="store_true",
                    help="fold-in serving benchmark instead of the training sweep")
     p.add_argument("--serve-sweeps", type=int, default=30)
@@ -254,7 +274,7 @@ def run_sharded(args, world, rank, local):
             "metric": METRIC, "value": N * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "tokens": N, "docs": info.num_docs, "vocab": info.vocab, "K": K,
+            "config": {"workload": workload(args.preset), "tokens": N, "docs": info.num_docs, "vocab": info.vocab, "K": K,
                        "dense_words": info.num_dense, "chunks": info.num_chunks,
                        "l2": "inputs_larger_than_l2 (resident corpus ~1.6 GB per sweep pass)",
                        "parallelism": f"doc-sharded x{world}: chunks {st.ranges}, NCCL topic broadcast per sweep"},
@@ -285,7 +305,10 @@ def run_ours(args, world, rank, local):
     info = corpus.info
     K = info.K_hint
     N = info.num_tokens
-    tr = L.Trainer(corpus, K=K, seed=42, device=local)
+    tr = L.Trainer(corpus, K=K, seed=42, device=local, alpha=ALPHA.get(args.preset),
+                   device_budget=int(args.budget_gb * 2**30), stream_mode=2 if args.stream else 0,
+                   num_streams=4 if args.stream else 0)
+    streaming, n_streams, _ = tr.stream_info()
     stream = torch.cuda.current_stream()
     tr.set_stream(stream.cuda_stream)
     z0 = corpus.topics()
@@ -363,6 +386,8 @@ def run_ours(args, world, rank, local):
     alg_bytes = sampler_algorithmic_bytes(cnt, K, dense_words_per_sweep, sweeps, launches_sample)
     ms_per_launch = tm.ms_sample / max(launches_sample, 1)
     achieved = alg_bytes / launches_sample / (ms_per_launch / 1e3) / 1e9 if launches_sample else None
+    if streaming:
+        achieved = None  # the timed stage spans the chunk copies, doc-row rebuilds and sampling
     peaks, peak_src = measured_peaks()
     peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
     traffic = ncu_traffic()
@@ -399,10 +424,13 @@ def run_ours(args, world, rank, local):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": sweeps,
             "warmup": args.warmup, "ms_per_step": ms / sweeps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "tokens": N, "docs": info.num_docs, "vocab": info.vocab,
-                       "K": K, "dense_words": info.num_dense, "chunks": info.num_chunks,
-                       "l2": "inputs_larger_than_l2 (resident corpus ~1.6 GB per sweep pass)",
-                       "parallelism": "single GPU"},
+            "config": {"workload": workload(args.preset), "tokens": N, "docs": info.num_docs, "vocab": info.vocab,
+                       "K": K, "alpha": tr.alpha, "dense_words": info.num_dense, "chunks": info.num_chunks,
+                       "l2": "inputs_larger_than_l2 (the corpus pass per sweep exceeds the 126 MB L2)",
+                       "parallelism": "single GPU",
+                       "chunks_streamed": (f"{n_streams} streams, {tr.stream_info()[2] / 2**30:.1f} GiB "
+                                           f"copied host->device in total") if streaming else "no (resident)",
+                       "device_bytes": tr.device_bytes},
             "loglik_per_token": ll_mean,
             "ms_per_step_with_ll": ms_ll_sweep,
             "e2e": e2e,
@@ -414,7 +442,9 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_launch": alg_bytes / max(launches_sample, 1),
                          "ms_per_launch": ms_per_launch},
             "stages_ms_per_sweep": {"wt": tm.ms_wt / sweeps, "stats": tm.ms_stats / sweeps,
-                                    "dt": tm.ms_dt / sweeps, "sample": tm.ms_sample / sweeps},
+                                    "dt": tm.ms_dt / sweeps, "sample": tm.ms_sample / sweeps,
+                                    "note": ("streamed: 'sample' spans copies, doc-row rebuilds and sampling "
+                                             "of all chunks on their streams") if streaming else ""},
             "sweep_ms_trace": trace,
             "sweep_counters": {"early_accept_frac": cnt.early_accept / max(cnt.tokens, 1),
                                "mean_nnz_full": cnt.sum_nnz_full / max(cnt.full, 1),
@@ -595,11 +625,72 @@ def run_serving(args, local):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, local):
+    """Batched training: args.batch_models independent corpora (K from {16,...,256}, D in
+    [100,5000], V in [1000,20000], Poisson(80) lengths, 16 generating topics), each for
+    args.batch_sweeps sweeps.  Plain: every model on its own trainer, one after another.
+    Batched: the same models in one batch, autotuned, all sweeps in one graph launch.
+    Every model's final topics must agree between the two."""
+    from concurrent.futures import ThreadPoolExecutor
+    import numpy as np
+    import torch
+    import lda_sc20_b200 as L
+    from lda_sc20_b200.batch import Batch, batch_corpus_configs
+
+    torch.cuda.set_device(local)
+    cfgs = batch_corpus_configs(args.batch_models)
+    with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
+        corpora = list(ex.map(L.Corpus.generate, cfgs))
+    Ks = [g.K for g in cfgs]
+    N = [c.info.num_tokens for c in corpora]
+    total = int(sum(N))
+    sweeps = args.batch_sweeps
+    clocks = ClockSampler(physical_gpu(local))
+    clocks.start()
+    plain = [L.Trainer(c, K=K, seed=11 + i, device=local) for i, (c, K) in enumerate(zip(corpora, Ks))]
+    plain[0].iterate(1)                       # warm-up launch, then back to sweep 0
+    plain[0].set_topics(corpora[0].topics())
+    plain[0].iteration = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ll_plain = [t.iterate(sweeps, ll=True) for t in plain]
+    plain_s = time.perf_counter() - t0
+    batched = [L.Trainer(c, K=K, seed=11 + i, device=local) for i, (c, K) in enumerate(zip(corpora, Ks))]
+    b = Batch(batched)
+    t0 = time.perf_counter()
+    tuning, tuned_ms = b.autotune(sweeps_per_trial=2)
+    tune_s = time.perf_counter() - t0
+    l0, _ = b.stats()
+    t0 = time.perf_counter()
+    ll_b = b.iterate(sweeps, ll=True)
+    batch_s = time.perf_counter() - t0
+    l1, work = b.stats()
+    clk = clocks.stop()
+    same = sum(int(np.array_equal(p.topics(), q.topics())) for p, q in zip(plain, batched))
+    ll_rel = max(abs(x - y) / abs(y) for x, y in zip(ll_b, ll_plain))
+    line = {"metric": "batched_gibbs_tokens_per_s_per_iter", "value": total * sweeps / batch_s, "unit": "tokens/s",
+            "n_gpus": 1, "steps": sweeps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"{len(corpora)} independent corpora: K in {{16,32,64,128,256}}, D~U[100,5000], "
+                                   f"V~U[1000,20000], len~Poisson(80), 16 generating topics, alpha=50/K, beta=0.01; "
+                                   f"{sweeps} sweeps each", "models": len(corpora), "tokens": total},
+            "plain_sequential_tokens_per_s": total * sweeps / plain_s,
+            "batched_vs_plain": plain_s / batch_s,
+            "seconds": {"plain_sequential": plain_s, "batched": batch_s, "autotune": tune_s},
+            "autotune": {"warps": tuning[0], "schedule": ["largest_first", "model_major"][tuning[1]],
+                         "tile_tokens": tuning[2], "ms_per_sweep": tuned_ms},
+            "gpu_launches": l1 - l0, "work_items_per_sweep": work,
+            "models_identical_to_plain": f"{same}/{len(corpora)}", "loglik_max_rel_diff": ll_rel,
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     world, rank, local = dist_setup(args)
     if args.serve:
         return run_serving(args, local)
+    if args.batch:
+        return run_batch(args, local)
     if args.impl == "reference":
         run_reference(args, world, rank, local)
     else:

@@ -132,6 +132,8 @@ typedef struct {
     int32_t stream_mode;    /* 0: keep the corpus resident when it fits device_budget, else
                                stream it; 1: always resident; 2: always stream */
     int32_t num_streams;    /* streaming: CUDA streams = chunk slots on the device (0: 4) */
+    int32_t num_dense;      /* 0: the corpus' dense/sparse split; n > 0: words [0, n) use the
+                               dense word-topic path; -1: none (results do not depend on it) */
 } lda_train_config;
 
 /* Sweep counters accumulated since the trainer was created or lda_trainer_reset_stats. */
@@ -296,6 +298,35 @@ typedef struct {
  * different streams or devices sharing a context) race; serialise them.  The call is
  * asynchronous on `stream` (NULL: the legacy default stream) and sets `device` current. */
 int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream);
+
+/* ------------------------------------------------ batched training */
+/* No counterpart in the reference (EZLDA trains one corpus per process).  A batch sweeps
+ * many resident trainers together: per stage, one persistent kernel takes work items of
+ * every model from a shared list (each model keeps its own K, alpha, beta, seed and device
+ * arrays), and the sweeps of one lda_batch_iterate call are one CUDA graph launch.  Every
+ * model's topics after a batched sweep equal its own trainer's after the same sweep.  The
+ * batch owns its trainers' state while it exists: sweeping a trainer on its own in between
+ * makes lda_batch_iterate fail with LDA_ERR_STATE. */
+typedef struct lda_batch lda_batch;
+typedef struct {
+    int32_t warps;        /* warps per CTA of the batched kernels, 1..8 */
+    int32_t schedule;     /* 0: largest work items first across models; 1: model by model */
+    int32_t tile_tokens;  /* tokens per sampler work item (>= 32): warps per frequent word */
+} lda_batch_tuning;
+/* tuning NULL: {8, 0, 512}.  The trainers must outlive the batch. */
+int lda_batch_create(lda_trainer* const* trainers, int32_t n, const lda_batch_tuning* tuning, lda_batch** out);
+int lda_batch_destroy(lda_batch* b);
+int lda_batch_set_tuning(lda_batch* b, const lda_batch_tuning* tuning);
+int lda_batch_get_tuning(const lda_batch* b, lda_batch_tuning* tuning);
+/* `sweeps` sweeps of every model in one graph launch; with ll_mode the FP64 LL of the last
+ * sweep per model (lda_batch_loglik, and each trainer's lda_trainer_loglik). */
+int lda_batch_iterate(lda_batch* b, int32_t sweeps, int32_t ll_mode);
+int lda_batch_loglik(const lda_batch* b, double* ll /*n*/, int32_t n);
+int lda_batch_stats(const lda_batch* b, int64_t* kernel_launches, int64_t* work_items);
+/* Times every candidate tuning (warps {4,8} x schedule {0,1} x tile_tokens {128,256,512})
+ * for sweeps_per_trial sweeps on the live batch, restoring the models' topics, iterations
+ * and counters after each trial, and keeps the fastest. */
+int lda_batch_autotune(lda_batch* b, int32_t sweeps_per_trial, lda_batch_tuning* best, double* best_ms_per_sweep);
 
 /* ------------------------------------------------ fold-in serving */
 /* No counterpart in the reference: EZLDA trains only.  A model is the frozen word side

@@ -191,12 +191,12 @@ class Trainer:
 
     def __init__(self, corpus: Corpus, K: int, alpha: float | None = None, beta: float = 0.01,
                  seed: int = 42, device: int = 0, device_budget: int = 0, stream_mode: int = 0,
-                 num_streams: int = 0):
+                 num_streams: int = 0, num_dense: int = 0):
         self._lib = load()
         if alpha is None:
             alpha = 50.0 / K  # EZLDA/Argument.cuh:9
         cfg = TrainConfig(K=K, alpha=alpha, beta=beta, seed=seed, device=device, device_budget=device_budget,
-                          stream_mode=stream_mode, num_streams=num_streams)
+                          stream_mode=stream_mode, num_streams=num_streams, num_dense=num_dense)
         h = C.c_void_p()
         check(self._lib.lda_trainer_create(corpus._h, C.byref(cfg), C.byref(h)))
         self._h = h

@@ -46,8 +46,12 @@ class TrainConfig(C.Structure):
     _fields_ = [
         ("K", C.c_int32), ("alpha", C.c_float), ("beta", C.c_float), ("seed", C.c_uint64),
         ("device", C.c_int32), ("device_budget", C.c_int64), ("stream_mode", C.c_int32),
-        ("num_streams", C.c_int32),
+        ("num_streams", C.c_int32), ("num_dense", C.c_int32),
     ]
+
+
+class BatchTuning(C.Structure):
+    _fields_ = [("warps", C.c_int32), ("schedule", C.c_int32), ("tile_tokens", C.c_int32)]
 
 
 class SweepCounters(C.Structure):
@@ -138,6 +142,14 @@ SIGNATURES = {
     "lda_server_get_topics": (I32, [P, U32, P, I32]),
     "lda_trainer_stream_info": (I32, [P, P, P, P]),
     "lda_corpus_generate_requests": (I32, [P, U64, I64, F64, F64, I32, I32, P, P, I64]),
+    "lda_batch_create": (I32, [P, I32, P, P]),
+    "lda_batch_destroy": (I32, [P]),
+    "lda_batch_set_tuning": (I32, [P, P]),
+    "lda_batch_get_tuning": (I32, [P, P]),
+    "lda_batch_iterate": (I32, [P, I32, I32]),
+    "lda_batch_loglik": (I32, [P, P, I32]),
+    "lda_batch_stats": (I32, [P, P, P]),
+    "lda_batch_autotune": (I32, [P, I32, P, P]),
     "lda_server_set_item_tokens": (I32, [P, I32]),
     "lda_server_stats": (I32, [P, P, P]),
     "lda_serve_replay": (I32, [P, I32, P, P, P, P, P, P]),

@@ -23,7 +23,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-I" + INC]
 
-LIB_SOURCES = ["trainer.cu", "serving.cu", "corpus.cpp"]
+LIB_SOURCES = ["trainer.cu", "serving.cu", "batch.cu", "corpus.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -23,6 +23,7 @@
 
 #include "common.h"
 #include "device_common.cuh"
+#include "launch_util.h"
 
 using namespace lda;
 
@@ -416,7 +417,7 @@ extern "C" int lda_model_from_trainer(lda_trainer* t, int64_t device_budget, lda
     a.swt_ent = src.swt_ent;
     a.phi = m->phi;
     const size_t smem = sizeof(float) * (size_t)m->K;
-    CUDA_TRY(cudaFuncSetAttribute((const void*)dev::k_phi_dense, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(raise_smem_limit((const void*)dev::k_phi_dense, smem));
     const int grid = (int)std::min<int64_t>(4096, (m->V + 7) / 8);
     dev::k_phi_dense<<<grid, 256, smem, stream>>>(a);
     CUDA_TRY(cudaGetLastError());
@@ -645,7 +646,7 @@ extern "C" int lda_server_create(lda_model* m, int64_t max_tokens, int32_t max_a
     s->warps = (int)std::min<int64_t>(8, (int64_t)max_smem / per_warp);
     if (s->warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", m->K);
     s->smem = (size_t)(s->warps * per_warp);
-    CUDA_TRY(cudaFuncSetAttribute((const void*)dev::k_foldin, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s->smem));
+    CUDA_TRY(raise_smem_limit((const void*)dev::k_foldin, s->smem));
     CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)dev::k_foldin, 32 * s->warps, s->smem));
     s->grid = std::max(1, per_sm * num_sms);
     CUDA_TRY(cudaStreamSynchronize(s->st));

@@ -1,0 +1,400 @@
+// sweep_body.cuh -- per-unit bodies of the sweep kernels (one word tile, one word, one
+// doc, one sampler tile), shared by the single-corpus kernels and the batched ones.
+//
+// Every float operation below is an explicit round-to-nearest intrinsic, so the compiler
+// cannot contract or reorder it.  The sampling arithmetic (summation orders, bin order,
+// tie rules) is the specification the CPU oracle restates; the CUDA path and the oracle
+// therefore draw identical topics for identical (seed, iteration, token).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_common.cuh"
+
+namespace lda {
+namespace dev {
+
+// ---------------------------------------------------------------- WT rebuild
+// Warp per word tile: the tile's topics are histogrammed in a warp-private shared row
+// (match_any-aggregated shared atomics, so a word whose tokens share a topic costs one
+// atomic per distinct topic per 32 tokens).  Dense tiles add their row into the dense
+// word-topic matrix; a sparse word (one tile over all chunks) is compacted to
+// (k<<16 | count) ascending k.  Topic totals n_k are privatised per CTA and flushed once.
+// Replaces WTDen_Update_Kernel, WT_Update_Kernel, sparseMatrixAdd and
+// WTDen_Sum_Update_Kernel (EZLDA/utility.cu:1067-1102, :10-76, :1132-1204, :1104-1126).
+struct WtArgs {
+    const int4* tiles;  // {word, start, count, dense}
+    int ntiles;
+    unsigned* tile_counter;
+    const uint16_t* z;
+    int K, V, Vd, C;
+    const uint32_t* seg_off;  // [C*V]
+    const uint32_t* seg_cnt;  // [C*V]
+    int* dwt;                 // [Vd*K]
+    const uint32_t* swt_off;  // [V-Vd]
+    uint32_t* swt_nnz;
+    uint32_t* swt_ent;
+    int* n_k;
+    int* err;
+};
+
+// One word tile: histogram its topics in the warp's shared row `hist` (zero on entry and
+// on exit) and add it to the dense row or write the sparse row; topic totals go to `nk`
+// (a CTA-private shared array, or the model's global totals).
+__device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t* hist, unsigned* nk, int lane) {
+    const int w = t.x;
+    if (t.w & 1) {
+        hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, a.K, lane, a.err);
+    } else {
+        for (int c = 0; c < a.C; ++c) {
+            const size_t idx = (size_t)c * a.V + w;
+            hist_segment(a.z, a.seg_off[idx], a.seg_cnt[idx], hist, a.K, lane, a.err);
+        }
+    }
+    __syncwarp();
+    if (t.w & 1) {
+        int* row = a.dwt + (size_t)w * a.K;
+        for (int k = lane; k < a.K; k += 32) {
+            const uint32_t h = hist[k];
+            if (h) {
+                atomicAdd(row + k, (int)h);
+                atomicAdd(nk + k, h);
+                hist[k] = 0u;
+            }
+        }
+    } else {
+        const int s = w - a.Vd;
+        uint32_t* out = a.swt_ent + a.swt_off[s];
+        uint32_t nnz = 0;
+        for (int kb = 0; kb < a.K; kb += 32) {
+            const int k = kb + lane;
+            const uint32_t h = k < a.K ? hist[k] : 0u;
+            const unsigned b = __ballot_sync(FULL, h != 0u);
+            if (h) {
+                out[nnz + __popc(b & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+                atomicAdd(nk + k, h);
+                hist[k] = 0u;
+            }
+            nnz += (uint32_t)__popc(b);
+        }
+        if (lane == 0) a.swt_nnz[s] = nnz;
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------- word stats
+// Warp per word: max / 2nd / 3rd topic of phi (ties to the lower k), phi at those
+// topics, and the 32 lane partials of Q = alpha * sum_{k != max} phi_k.  Replaces
+// MaxTopicDense_Update_Kernel / MaxTopicSparse_Update_Kernel (EZLDA/utility.cu:305-1062).
+struct StatsArgs {
+    int V, Vd, K;
+    float alpha, beta, Vbeta;
+    const int* n_k;
+    const int* dwt;
+    const uint32_t* swt_off;
+    const uint32_t* swt_nnz;
+    const uint32_t* swt_ent;
+    uint32_t* st_top2;  // (k2 << 16) | maxK
+    uint32_t* st_k3;
+    float4* st_phi;     // {phi_max, phi_2nd, phi_3rd, Q}
+    float* st_ql;       // [V*32]
+};
+
+// Statistics of word w from its column (built into the warp's shared `col`).
+__device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const float* r, float* col, int lane) {
+    build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, nullptr);
+    float v1 = -1.0f;
+    int k1 = 0x7fffffff;
+    for (int k = lane; k < a.K; k += 32) if (col[k] > v1) { v1 = col[k]; k1 = k; }
+    warp_argmax(v1, k1);
+    float v2 = -1.0f;
+    int k2 = 0x7fffffff;
+    for (int k = lane; k < a.K; k += 32) if (k != k1 && col[k] > v2) { v2 = col[k]; k2 = k; }
+    warp_argmax(v2, k2);
+    float v3 = -1.0f;
+    int k3 = 0x7fffffff;
+    for (int k = lane; k < a.K; k += 32) if (k != k1 && k != k2 && col[k] > v3) { v3 = col[k]; k3 = k; }
+    warp_argmax(v3, k3);
+    float ql = 0.0f;
+    for (int k = lane; k < a.K; k += 32) if (k != k1) ql = ffma(a.alpha, col[k], ql);
+    const float qp = warp_ks_scan(ql, lane);
+    const float Q = __shfl_sync(FULL, qp, 31);
+    a.st_ql[(size_t)w * 32 + lane] = ql;
+    if (lane == 0) {
+        a.st_top2[w] = ((uint32_t)k2 << 16) | (uint32_t)k1;
+        a.st_k3[w] = (uint32_t)k3;
+        a.st_phi[w] = make_float4(v1, v2, v3, Q);
+    }
+    __syncwarp();
+}
+
+// ---------------------------------------------------------------- DT rebuild
+// Warp per doc of one chunk: the doc's topics are gathered through the doc-order ->
+// word-sorted map into a warp-private shared histogram, each token's counts of its
+// word's max / 2nd topic are scattered to its word-sorted slot, and the histogram is
+// compacted to (k<<16 | count) ascending k.  Replaces DT_Update_Kernel
+// (EZLDA/utility.cu:79-284).
+struct DtArgs {
+    uint32_t d_begin, d_end;
+    int K;
+    const uint32_t* doc_off;    // [D+1] doc-order token offsets
+    const uint32_t* dtok_pos;   // [N]
+    const uint32_t* dtok_word;  // [N]
+    const uint16_t* z;
+    const uint32_t* st_top2;
+    const uint32_t* dt_off;
+    uint32_t* dt_nnz;
+    uint32_t* dt_ent;
+    uint32_t* meta;             // [N] word-sorted: (n_d,2nd << 16) | n_d,max
+    int* err;
+    // dtok_pos / dtok_word / meta hold tokens [tok_base, ...) and dt_ent the doc-row
+    // entries [dt_base, ...): 0 when the whole corpus is resident, the chunk's first token
+    // and first doc-row entry when the chunk is streamed into a slot buffer
+    uint32_t tok_base, dt_base;
+};
+
+// Doc d: its counts in the warp's shared `hist` (zero on entry and on exit), the
+// per-token metadata and the compacted row.
+__device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hist, int lane) {
+    const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
+    for (uint32_t base = 0; base < n; base += 32) {
+        bool valid = base + lane < n;
+        uint32_t k = valid ? (uint32_t)__ldg(a.z + __ldg(a.dtok_pos + (b - a.tok_base) + base + lane)) : 0xffffffffu;
+        if (valid && k >= (uint32_t)a.K) {
+            atomicOr(a.err, 1);
+            valid = false;
+            k = 0xfffffffeu;
+        }
+        const unsigned m = __match_any_sync(FULL, k);
+        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < n; i += 32) {
+        const uint32_t pos = __ldg(a.dtok_pos + (b - a.tok_base) + i);
+        const uint32_t t2 = __ldg(a.st_top2 + __ldg(a.dtok_word + (b - a.tok_base) + i));
+        const uint32_t k1 = t2 & 0xffffu, k2 = t2 >> 16;
+        const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
+        a.meta[pos - a.tok_base] = (c2 << 16) | c1;
+    }
+    __syncwarp();
+    uint32_t* out = a.dt_ent + (__ldg(a.dt_off + d) - a.dt_base);
+    uint32_t nnz = 0;
+    for (int kb = 0; kb < a.K; kb += 32) {
+        const int k = kb + lane;
+        const uint32_t h = k < a.K ? hist[k] : 0u;
+        const unsigned bal = __ballot_sync(FULL, h != 0u);
+        if (h) {
+            out[nnz + __popc(bal & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+            hist[k] = 0u;
+        }
+        nnz += (uint32_t)__popc(bal);
+    }
+    if (lane == 0) a.dt_nnz[d] = nnz;
+    __syncwarp();
+}
+
+// ------------------------------------------------------------------- sampler
+// Warp per (word, token range) tile.  The word's phi column (phi_max zeroed) sits in
+// warp-private shared memory.  Each 32-token group is screened thread-per-token by the
+// max-topic bound.  Tokens the bound does not settle (all tokens in LL mode) are then
+// evaluated one at a time by the whole warp, with uniform control flow:
+//   S      lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
+//          one Kogge-Stone scan gives the lane prefixes; a doc row is evaluated once
+//          for consecutive tokens of the same (word, doc) in the tile;
+//   bucket a ballot over the lane prefixes picks the block of an S-bucket draw; the
+//          in-block draw (at most B entries) runs afterwards thread-per-token, all the
+//          group's S-bucket tokens at once;
+//   Q      a ballot over the per-word lane prefixes of Q, then one topic per lane with a
+//          scan and a ballot (topics k = l, l+32, ..., 32 per round, carried).
+// Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain
+// (EZLDA/utility.cu:2680-3312, :1625-2103, :1217-1611) in one pass, with no
+// effective-token list in global memory and no spin lock.
+struct SampleArgs {
+    const int4* tiles;  // {word, start, count, dense}
+    int ntiles;
+    unsigned* tile_counter;
+    double* tile_ll;
+    int K, Vd, ll_mode;
+    float alpha, beta, Vbeta;
+    double den_add;  // (double)K * (double)alpha
+    uint32_t seed_lo, seed_hi, iter;
+    const int* n_k;
+    const int* dwt;
+    const uint32_t* swt_off;
+    const uint32_t* swt_nnz;
+    const uint32_t* swt_ent;
+    const uint32_t* st_top2;
+    const float4* st_phi;
+    const float* st_ql;
+    const uint32_t* tok_doc;
+    const uint32_t* meta;
+    uint16_t* z;
+    const uint32_t* doc_len;
+    const uint32_t* dt_off;
+    const uint32_t* dt_nnz;
+    const uint32_t* dt_ent;
+    // tokens, ea, full, sum_nnz, max, s, q, word_nnz, dense tiles, sparse tiles, rows, row entries
+    unsigned long long* ctr;
+    // tok_doc / meta hold tokens [tok_base, ...) and dt_ent the doc-row entries
+    // [dt_base, ...) (non-zero when the chunk is streamed into a slot buffer)
+    uint32_t tok_base, dt_base;
+};
+
+// Sweep counters live in shared memory (one row per warp, written by lane 0) so they
+// cost no registers in the sampling loop.
+enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE, C_ROWS, C_RENT, C_NUM };
+
+#ifndef LDA_SAMPLE_MIN_BLOCKS
+#define LDA_SAMPLE_MIN_BLOCKS 4
+#endif
+
+// Branch taken by a token (counters only).
+enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
+
+// One sampler tile (tile index `tile` of a.tiles, content t) with the word column in the
+// warp's shared `col`, the reciprocal table `r` and the warp's shared counter row `ctr`.
+template <bool LL>
+__device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
+                                            const float* r, float* col, uint32_t* ctr, int lane) {
+    const int w = t.x;
+    const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
+    __syncwarp();
+    uint32_t wnnz = 0;
+    build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
+    if (lane == 0) {
+        ctr[C_WNNZ] += wnnz;
+        ctr[w < a.Vd ? C_TDENSE : C_TSPARSE] += 1u;
+    }
+    const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
+    const float4 ph = __ldg(a.st_phi + w);
+    const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
+    const float QP = warp_ks_scan(QL, lane);
+    const float Q = __shfl_sync(FULL, QP, 31);
+    if (lane == 0) col[maxK] = 0.0f;
+    __syncwarp();
+    double ll = 0.0;
+    uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
+    const uint32_t* row = a.dt_ent;
+    float SL = 0.0f, SP = 0.0f, S = 0.0f;
+    for (uint32_t g = 0; g < cnt; g += 32) {
+        const bool valid = g + lane < cnt;
+        const uint32_t tok = start + g + lane;
+        uint32_t d = 0xffffffffu, nd = 0, my_nnz = 0, my_off = 0;
+        float u = 0.0f, pmax = 0.0f;
+        bool ea = false;
+        if (valid) {
+            d = __ldg(a.tok_doc + (tok - a.tok_base));
+            const uint32_t m = __ldg(a.meta + (tok - a.tok_base));
+            nd = __ldg(a.doc_len + d);
+            my_nnz = __ldg(a.dt_nnz + d);
+            my_off = __ldg(a.dt_off + d) - a.dt_base;
+            const uint32_t cmax = m & 0xffffu, c2 = m >> 16;
+            u = token_uniform(a.seed_lo, a.seed_hi, iter, tok);
+            pmax = fmul(fadd(u2f(cmax), a.alpha), ph.x);
+            const float shat = ffma(u2f(c2), ph.y, fmul(u2f(nd - cmax - c2), ph.z));
+            const float bound = fadd(fadd(pmax, shat), Q);
+            ea = fmul(u, bound) < pmax;
+        }
+        int znew = maxK;
+        // per-lane record of this token's evaluation, for the deferred draw and counters
+        const uint32_t* my_row = row;
+        uint32_t my_b0 = 0, my_b1 = 0;
+        float my_t2 = 0.0f;
+        int kind = BR_NONE;
+        bool evaluated = false;
+        const unsigned vmask = __ballot_sync(FULL, valid);
+        const unsigned emask = __ballot_sync(FULL, ea);
+        const unsigned need0 = LL ? vmask : (vmask & ~emask);
+        unsigned need = need0;
+        while (need) {
+            const int j = __ffs(need) - 1;
+            need &= need - 1u;
+            const uint32_t dj = __shfl_sync(FULL, d, j);
+            if (dj != cur) {
+                cur = dj;
+                nnz = __shfl_sync(FULL, my_nnz, j);
+                row = a.dt_ent + __shfl_sync(FULL, my_off, j);
+                B = (nnz + 31u) >> 5;
+                const uint32_t b0 = min(lane * B, nnz);
+                SL = block_mass(row, b0, min(b0 + B, nnz), col);
+                SP = warp_ks_scan(SL, lane);
+                S = __shfl_sync(FULL, SP, 31);
+                evaluated |= (lane == j);
+            }
+            const float pmj = __shfl_sync(FULL, pmax, j);
+            const float uj = __shfl_sync(FULL, u, j);
+            const float pS = fadd(pmj, S);
+            const float total = fadd(pS, Q);
+            if (LL) {
+                if (lane == j) ll += log((double)total / ((double)nd + a.den_add));
+            }
+            if (LL && ((emask >> j) & 1u)) continue;
+            const float target = fmul(uj, total);
+            if (target < pmj) {
+                if (lane == j) kind = BR_MAX;
+            } else if (target < pS) {
+                const float tt = fsub(target, pmj);
+                const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
+                const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
+                const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
+                if (lane == j) {
+                    kind = BR_S;
+                    my_row = row;
+                    my_b0 = (uint32_t)ls * B;
+                    my_b1 = min(my_b0 + B, nnz);
+                    my_t2 = ls > 0 ? fsub(tt, prev) : tt;
+                }
+            } else {
+                const float tt = fsub(target, pS);
+                const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
+                const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
+                const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
+                const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
+                const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                const int K = a.K;
+                const float alpha = a.alpha;
+                const uint32_t n = (uint32_t)((K - ls + 31) / 32);
+                const int zq = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                    const int k = ls + 32 * (int)i;
+                    const float cz = col[k];
+                    key = k;
+                    term = fmul(alpha, cz);
+                    ok = cz > 0.0f;
+                });
+                if (lane == j) {
+                    kind = BR_Q;
+                    znew = zq;
+                }
+            }
+        }
+        if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, col, my_t2, maxK);
+        if (valid) a.z[tok] = (uint16_t)znew;
+        // counters of the group: ballots and warp sums instead of per-token updates
+        const bool in_need = (need0 >> lane) & 1u;
+        const unsigned sm = __ballot_sync(FULL, kind == BR_S), qm = __ballot_sync(FULL, kind == BR_Q);
+        const unsigned xm = __ballot_sync(FULL, kind == BR_MAX), rm = __ballot_sync(FULL, evaluated);
+        const uint32_t nnz_full = __reduce_add_sync(FULL, in_need ? my_nnz : 0u);
+        const uint32_t nnz_rows = __reduce_add_sync(FULL, evaluated ? my_nnz : 0u);
+        if (lane == 0) {
+            ctr[C_TOK] += __popc(vmask);
+            ctr[C_EA] += __popc(emask);
+            ctr[C_FULL] += __popc(need0);
+            ctr[C_NNZ] += nnz_full;
+            ctr[C_MAX] += __popc(xm) + __popc(emask);
+            ctr[C_S] += __popc(sm);
+            ctr[C_Q] += __popc(qm);
+            ctr[C_ROWS] += __popc(rm);
+            ctr[C_RENT] += nnz_rows;
+        }
+    }
+    if (LL) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);
+        if (lane == 0) a.tile_ll[tile] = ll;
+    }
+}
+
+}  // namespace dev
+}  // namespace lda

@@ -17,6 +17,8 @@
 
 #include "common.h"
 #include "kernels.cuh"
+#include "launch_util.h"
+#include "trainer_internal.h"
 
 using namespace lda;
 
@@ -79,6 +81,7 @@ struct lda_trainer {
     bool ll_valid = false;
     std::vector<bool> chunk_sampled_ll;
     int chunk_first = 0, chunk_last = 0;  // sampled chunk range of lda_trainer_iterate
+    std::vector<int4> h_stiles, h_wtiles;  // host copies of the tile lists
 
     // streaming: the per-token arrays of the doc-topic rebuild and the sampler (doc of each
     // token, doc-order -> word-sorted map and word, per-token metadata) and the doc rows
@@ -212,6 +215,16 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, T.device));
     T.K = cfg->K; T.alpha = cfg->alpha; T.beta = cfg->beta; T.seed = cfg->seed;
     T.N = c->N; T.V = c->V; T.D = c->D; T.C = c->C; T.Vd = c->V_dense;
+    if (cfg->num_dense != 0) {
+        // words are frequency ranks, so any prefix can take the dense path; sparse rows
+        // pack counts in 16 bits
+        const int64_t nd = cfg->num_dense < 0 ? 0 : cfg->num_dense;
+        if (nd > T.V) return fail(LDA_ERR_ARG, "num_dense %d above the vocabulary (%lld)", cfg->num_dense, (long long)T.V);
+        if (nd < T.V && c->word_count[nd] > 65535)
+            return fail(LDA_ERR_ARG, "word %lld has %lld tokens: words above 65535 tokens must be dense", (long long)nd,
+                        (long long)c->word_count[nd]);
+        T.Vd = (int)nd;
+    }
     T.Vbeta = (float)T.V * T.beta;
     T.budget = cfg->device_budget;
     T.chunk_tok = c->chunk_tok;
@@ -374,13 +387,15 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     CUDA_TRY(cudaMemset(T.tile_ll, 0, sizeof(double) * std::max<size_t>(st.size(), 1)));
     if (!st.empty()) CUDA_TRY(cudaMemcpy(T.s_tiles, st.data(), sizeof(int4) * st.size(), cudaMemcpyHostToDevice));
     if (!wt.empty()) CUDA_TRY(cudaMemcpy(T.w_tiles, wt.data(), sizeof(int4) * wt.size(), cudaMemcpyHostToDevice));
+    T.h_stiles = st;
+    T.h_wtiles = wt;
 
     // ---- launch shapes: persistent grids sized by occupancy
     const int threads = 32 * T.warps;
     for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
                     std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair((const void*)dev::k_sample_t<false>, T.smem_sample),
                     std::make_pair((const void*)dev::k_sample_t<true>, T.smem_sample)})
-        CUDA_TRY(cudaFuncSetAttribute(kv.first, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kv.second));
+        CUDA_TRY(raise_smem_limit(kv.first, kv.second));
     if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
@@ -448,6 +463,24 @@ extern "C" int lda_trainer_device_bytes(const lda_trainer* t, int64_t* b) {
 
 // ------------------------------------------------------------------- stages
 
+static dev::WtArgs wt_args(const lda_trainer* t) {
+    dev::WtArgs a;
+    a.tiles = t->w_tiles; a.ntiles = t->n_wtiles; a.tile_counter = t->tile_ctr;
+    a.z = t->z; a.K = t->K; a.V = (int)t->V; a.Vd = t->Vd; a.C = t->C;
+    a.seg_off = t->seg_off; a.seg_cnt = t->seg_cnt;
+    a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
+    a.n_k = t->n_k; a.err = t->err;
+    return a;
+}
+
+static dev::StatsArgs stats_args(const lda_trainer* t) {
+    dev::StatsArgs a;
+    a.V = (int)t->V; a.Vd = t->Vd; a.K = t->K; a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
+    a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
+    a.st_top2 = t->st_top2; a.st_k3 = t->st_k3; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
+    return a;
+}
+
 extern "C" int lda_update_wt(lda_trainer* t) {
     if (!t) return fail(LDA_ERR_ARG, "null trainer");
     CUDA_TRY(cudaSetDevice(t->device));
@@ -455,12 +488,7 @@ extern "C" int lda_update_wt(lda_trainer* t) {
     CUDA_TRY(cudaMemsetAsync(t->n_k, 0, sizeof(int) * (size_t)t->K, t->stream));
     if (t->Vd > 0) CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
     CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
-    dev::WtArgs a;
-    a.tiles = t->w_tiles; a.ntiles = t->n_wtiles; a.tile_counter = t->tile_ctr;
-    a.z = t->z; a.K = t->K; a.V = (int)t->V; a.Vd = t->Vd; a.C = t->C;
-    a.seg_off = t->seg_off; a.seg_cnt = t->seg_cnt;
-    a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
-    a.n_k = t->n_k; a.err = t->err;
+    const dev::WtArgs a = wt_args(t);
     const int grid = std::max(1, std::min(t->grid_wt, (t->n_wtiles + t->warps - 1) / t->warps));
     dev::k_wt_build<<<grid, 32 * t->warps, t->smem_wt, t->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
@@ -472,10 +500,7 @@ extern "C" int lda_max_topic(lda_trainer* t) {
     if (!t) return fail(LDA_ERR_ARG, "null trainer");
     CUDA_TRY(cudaSetDevice(t->device));
     t->begin_stage(1);
-    dev::StatsArgs a;
-    a.V = (int)t->V; a.Vd = t->Vd; a.K = t->K; a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
-    a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
-    a.st_top2 = t->st_top2; a.st_k3 = t->st_k3; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
+    const dev::StatsArgs a = stats_args(t);
     dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     t->end_stage();
@@ -521,7 +546,7 @@ static int load_chunk(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
     return LDA_OK;
 }
 
-static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
+static dev::DtArgs dt_args(const lda_trainer* t, int chunk, int slot) {
     const ChunkBufs b = chunk_bufs(t, chunk, slot);
     dev::DtArgs a;
     a.d_begin = (uint32_t)t->chunk_doc[chunk]; a.d_end = (uint32_t)t->chunk_doc[chunk + 1]; a.K = t->K;
@@ -530,6 +555,11 @@ static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
     a.err = t->err;
     a.tok_base = b.tok_base;
     a.dt_base = b.dt_base;
+    return a;
+}
+
+static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
+    const dev::DtArgs a = dt_args(t, chunk, slot);
     const int64_t nd = a.d_end - a.d_begin;
     const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps - 1) / t->warps));
     dev::k_dt_build<<<grid, 32 * t->warps, t->smem_dt, q>>>(a);
@@ -537,13 +567,11 @@ static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
     return LDA_OK;
 }
 
-static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaStream_t q) {
+static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, int ll_mode) {
     const ChunkBufs b = chunk_bufs(t, chunk, slot);
     const int base = t->s_tile_base[chunk], n = t->s_tile_base[chunk + 1] - base;
-    unsigned* ctr = t->tile_ctr + 1 + chunk;
-    CUDA_TRY(cudaMemsetAsync(ctr, 0, sizeof(unsigned), q));
     dev::SampleArgs a;
-    a.tiles = t->s_tiles + base; a.ntiles = n; a.tile_counter = ctr; a.tile_ll = t->tile_ll + base;
+    a.tiles = t->s_tiles + base; a.ntiles = n; a.tile_counter = t->tile_ctr + 1 + chunk; a.tile_ll = t->tile_ll + base;
     a.K = t->K; a.Vd = t->Vd; a.ll_mode = ll_mode ? 1 : 0;
     a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
     a.den_add = (double)t->K * (double)t->alpha;
@@ -554,6 +582,13 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
     a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.ctr = t->ctr;
     a.tok_base = b.tok_base;
     a.dt_base = b.dt_base;
+    return a;
+}
+
+static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaStream_t q) {
+    const dev::SampleArgs a = sample_args(t, chunk, slot, ll_mode);
+    const int n = a.ntiles;
+    CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(unsigned), q));
     if (n > 0) {
         const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
         if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * t->warps, t->smem_sample, q>>>(a);
@@ -867,6 +902,48 @@ int lda::trainer_model_source(lda_trainer* t, ModelSource* o) {
     return LDA_OK;
 }
 
+int lda::trainer_view(lda_trainer* t, TrainerView* v) {
+    if (!t || !v) return fail(LDA_ERR_ARG, "null argument");
+    if (t->streaming) return fail(LDA_ERR_STATE, "a streaming trainer cannot join a batch");
+    v->wt = wt_args(t);
+    v->st = stats_args(t);
+    v->dt = dt_args(t, 0, 0);
+    v->dt.d_begin = 0;
+    v->dt.d_end = (uint32_t)t->D;
+    v->sm = sample_args(t, 0, 0, 0);
+    v->sm.ntiles = t->s_tile_base[t->C];
+    v->device = t->device;
+    v->K = t->K;
+    v->Vd = t->Vd;
+    v->warps = t->warps;
+    v->N = t->N;
+    v->V = t->V;
+    v->D = t->D;
+    v->n_k = t->n_k;
+    v->dwt = t->dwt;
+    v->dwt_count = (int64_t)t->Vd * t->K;
+    v->tile_ll = t->tile_ll;
+    v->n_stiles = t->s_tile_base[t->C];
+    v->n_wtiles = t->n_wtiles;
+    v->s_tiles = t->h_stiles;
+    v->w_tiles = t->h_wtiles;
+    return LDA_OK;
+}
+
+int lda::trainer_note_sweeps(lda_trainer* t, int n, int ll_mode, double ll_sum) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    t->iter += (uint32_t)n;
+    if (n > 0) {
+        for (int ch = 0; ch < t->C; ++ch) t->chunk_sampled_ll[ch] = ll_mode != 0;
+        if (ll_mode) {
+            t->last_ll = ll_sum;
+            t->last_ll_tokens = t->N;
+            t->ll_valid = true;
+        }
+    }
+    return LDA_OK;
+}
+
 extern "C" int lda_get_topic_totals(lda_trainer* t, int32_t* nk) {
     if (!t || !nk) return fail(LDA_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(t->device));
@@ -1020,7 +1097,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
     const size_t smem = (size_t)(warps + 1) * row + (size_t)warps * 16 * sizeof(uint32_t);
     const void* kfn = io->ll_mode ? (const void*)dev::k_sample_t<true> : (const void*)dev::k_sample_t<false>;
-    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_TRY(raise_smem_limit(kfn, smem));
     int grid = 0;
     if ((rc = occupancy_grid(kfn, 32 * warps, smem, num_sms, &grid))) return rc;
     grid = std::max(1, std::min(grid, (io->num_tiles + warps - 1) / warps));

@@ -284,3 +284,13 @@ def test_streaming_by_budget_and_stage_api():
     assert np.array_equal(stm.topics(), z)
     with pytest.raises(L.LdaError):
         stm.doc_rows()
+
+
+def test_trainers_of_different_k_coexist():
+    """A trainer created after another with a larger K must not lower the kernels' shared
+    memory limit below what the first one launches with."""
+    big = L.Trainer(L.Corpus.generate(L.corpus_config("c0", num_docs=200, vocab=500, K=1024)), K=1024)
+    small = L.Trainer(L.Corpus.generate(L.corpus_config("c0", num_docs=200, vocab=500, K=16)), K=16)
+    big.iterate(2, ll=True)
+    small.iterate(2, ll=True)
+    big.iterate(1)
