@@ -22,6 +22,8 @@ INC = os.path.join(ROOT, "include")
 NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-O3", "-I" + INC]
+# extra nvcc flags for tuning builds (e.g. LDA_NVFLAGS="-DLDA_SAMPLE_TILE=256")
+NVFLAGS += os.environ.get("LDA_NVFLAGS", "").split()
 
 LIB_SOURCES = ["trainer.cu", "serving.cu", "batch.cu", "corpus.cpp"]
 

@@ -122,9 +122,10 @@ template <bool LL>
 __global__ void __launch_bounds__(256) kb_sample(BatchArgs b) {
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* r = smf + (size_t)b.Kmax * 2 * wid;
+    const int per = b.Kmax + col_words(b.Kmax);
+    float* r = smf + (size_t)per * wid;
     float* col = r + b.Kmax;
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(smf + (size_t)b.Kmax * 2 * warps) + C_NUM * wid;
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smf + (size_t)per * warps) + C_NUM * wid;
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncwarp();
     const uint32_t done = *b.sweeps_done;
@@ -343,7 +344,7 @@ static int batch_build(lda_batch* b) {
     const int threads = 32 * tu.warps;
     b->smem_hist = (size_t)tu.warps * b->Kmax * 4;
     b->smem_stats = (size_t)tu.warps * b->Kmax * 8;
-    b->smem_sample = (size_t)tu.warps * (b->Kmax * 8 + dev::C_NUM * 4);
+    b->smem_sample = (size_t)tu.warps * ((b->Kmax + dev::col_words(b->Kmax)) * 4 + dev::C_NUM * 4);
     if ((rc = occupancy((const void*)dev::kb_wt, threads, b->smem_hist, b->num_sms, &b->grid_wt)) ||
         (rc = occupancy((const void*)dev::kb_stats, threads, b->smem_stats, b->num_sms, &b->grid_stats)) ||
         (rc = occupancy((const void*)dev::kb_dt, threads, b->smem_hist, b->num_sms, &b->grid_dt)) ||

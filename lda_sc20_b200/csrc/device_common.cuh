@@ -72,24 +72,33 @@ __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uin
 }
 
 // ------------------------------------------------------------ word columns
+// The sampler's shared word column stores topic k at k + k/32: the 32 topics k = l,
+// l+32, ..., l+992 that one Q-bucket round reads then fall in 32 different banks (a plain
+// layout puts them all in bank l).  col_words(K) floats hold a skewed column.
+__host__ __device__ __forceinline__ int col_skew(int k) { return k + (k >> 5); }
+__host__ __device__ __forceinline__ int col_words(int K) { return (K + (K >> 5) + 4) & ~3; }
+
 // phi_k = ((float)n_wk + beta) * r_k into a warp-private shared row (EZLDA builds the
-// same column as WTHead, utility.cu:1257-1269 sparse, :1698-1702 dense).
+// same column as WTHead, utility.cu:1257-1269 sparse, :1698-1702 dense); SKEW selects the
+// sampler's layout.
+template <bool SKEW = false>
 __device__ __forceinline__ void build_column(float* col, const float* r, int w, int Vd, int K, float beta,
                                              const int* __restrict__ dwt, const uint32_t* __restrict__ swt_off,
                                              const uint32_t* __restrict__ swt_nnz,
                                              const uint32_t* __restrict__ swt_ent, int lane, uint32_t* nnz_read) {
     if (w < Vd) {
         const int* row = dwt + (size_t)w * K;
-        for (int k = lane; k < K; k += 32) col[k] = fmul(fadd(__int2float_rn(__ldg(row + k)), beta), r[k]);
+        for (int k = lane; k < K; k += 32)
+            col[SKEW ? col_skew(k) : k] = fmul(fadd(__int2float_rn(__ldg(row + k)), beta), r[k]);
     } else {
-        for (int k = lane; k < K; k += 32) col[k] = fmul(beta, r[k]);
+        for (int k = lane; k < K; k += 32) col[SKEW ? col_skew(k) : k] = fmul(beta, r[k]);
         __syncwarp();
         const int s = w - Vd;
         const uint32_t off = __ldg(swt_off + s), nnz = __ldg(swt_nnz + s);
         for (uint32_t e = lane; e < nnz; e += 32) {
             const uint32_t en = __ldg(swt_ent + off + e);
             const uint32_t k = en >> 16;
-            col[k] = fmul(fadd(u2f(en & 0xffffu), beta), r[k]);
+            col[SKEW ? col_skew((int)k) : (int)k] = fmul(fadd(u2f(en & 0xffffu), beta), r[k]);
         }
         if (nnz_read && lane == 0) *nnz_read += nnz;
     }
@@ -135,19 +144,19 @@ __device__ __forceinline__ int warp_level2(uint32_t n, float t2, int fallback, i
 }
 
 // Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
-// loads of two entries are issued together).
+// loads of two entries are issued together); col in the sampler's skewed layout.
 __device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
                                             const float* col) {
     float acc = 0.0f;
     uint32_t q = b0;
     for (; q + 2 <= b1; q += 2) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 1);
-        acc = ffma(u2f(e0 & 0xffffu), col[e0 >> 16], acc);
-        acc = ffma(u2f(e1 & 0xffffu), col[e1 >> 16], acc);
+        acc = ffma(u2f(e0 & 0xffffu), col[col_skew((int)(e0 >> 16))], acc);
+        acc = ffma(u2f(e1 & 0xffffu), col[col_skew((int)(e1 >> 16))], acc);
     }
     if (q < b1) {
         const uint32_t e = __ldg(row + q);
-        acc = ffma(u2f(e & 0xffffu), col[e >> 16], acc);
+        acc = ffma(u2f(e & 0xffffu), col[col_skew((int)(e >> 16))], acc);
     }
     return acc;
 }
@@ -162,7 +171,7 @@ __device__ __forceinline__ int block_draw(const uint32_t* __restrict__ row, uint
     for (uint32_t q = b0; q < b1; ++q) {
         const uint32_t e = __ldg(row + q);
         const int k = (int)(e >> 16);
-        const float cz = col[k];
+        const float cz = col[col_skew(k)];
         acc = ffma(u2f(e & 0xffffu), cz, acc);
         if (cz > 0.0f) {
             last = k;

@@ -68,8 +68,8 @@ __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleA
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* r = smf;
-    float* col = smf + (size_t)a.K * (1 + wid);
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(smf + (size_t)a.K * (1 + warps)) + C_NUM * wid;
+    float* col = smf + a.K + (size_t)col_words(a.K) * wid;
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(smf + a.K + (size_t)col_words(a.K) * warps) + C_NUM * wid;
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();

@@ -253,7 +253,8 @@ enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE,
 enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 
 // One sampler tile (tile index `tile` of a.tiles, content t) with the word column in the
-// warp's shared `col`, the reciprocal table `r` and the warp's shared counter row `ctr`.
+// warp's shared `col` (col_words(K) floats, skewed layout), the reciprocal table `r` and
+// the warp's shared counter row `ctr`.
 template <bool LL>
 __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
                                             const float* r, float* col, uint32_t* ctr, int lane) {
@@ -261,7 +262,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
     const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
     __syncwarp();
     uint32_t wnnz = 0;
-    build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
+    build_column<true>(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
     if (lane == 0) {
         ctr[C_WNNZ] += wnnz;
         ctr[w < a.Vd ? C_TDENSE : C_TSPARSE] += 1u;
@@ -271,7 +272,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
     const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
     const float QP = warp_ks_scan(QL, lane);
     const float Q = __shfl_sync(FULL, QP, 31);
-    if (lane == 0) col[maxK] = 0.0f;
+    if (lane == 0) col[col_skew(maxK)] = 0.0f;
     __syncwarp();
     double ll = 0.0;
     uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
@@ -358,7 +359,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
                 const uint32_t n = (uint32_t)((K - ls + 31) / 32);
                 const int zq = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
                     const int k = ls + 32 * (int)i;
-                    const float cz = col[k];
+                    const float cz = col[col_skew(k)];
                     key = k;
                     term = fmul(alpha, cz);
                     ok = cz > 0.0f;

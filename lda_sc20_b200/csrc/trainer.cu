@@ -24,7 +24,10 @@ using namespace lda;
 
 namespace {
 
-constexpr int kSampleTile = 512;   // tokens per sampler tile (a word's column is rebuilt per tile)
+#ifndef LDA_SAMPLE_TILE
+#define LDA_SAMPLE_TILE 512
+#endif
+constexpr int kSampleTile = LDA_SAMPLE_TILE;  // tokens per sampler tile (a word's column is rebuilt per tile)
 constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
 constexpr int kCounters = 16;
 
@@ -233,8 +236,11 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     const int64_t row = (int64_t)T.K * 4;
     T.warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
+    auto sample_bytes = [&](int w) { return (size_t)T.K * 4 + (size_t)w * (dev::col_words(T.K) * 4 + 16 * sizeof(uint32_t)); };
+    while (T.warps > 1 && sample_bytes(T.warps) > (size_t)max_smem) --T.warps;
+    if (sample_bytes(T.warps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
     T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
-    T.smem_sample = (size_t)(T.warps + 1) * row + (size_t)T.warps * 16 * sizeof(uint32_t);
+    T.smem_sample = sample_bytes(T.warps);
     T.smem_dt = (size_t)T.warps * row;
 
     // ---- host-side derived layout
@@ -1095,7 +1101,8 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     const int64_t row = (int64_t)io->K * 4;
     const int warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
-    const size_t smem = (size_t)(warps + 1) * row + (size_t)warps * 16 * sizeof(uint32_t);
+    const size_t smem = (size_t)io->K * 4 + (size_t)warps * (dev::col_words(io->K) * 4 + 16 * sizeof(uint32_t));
+    if (warps < 1 || smem > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
     const void* kfn = io->ll_mode ? (const void*)dev::k_sample_t<true> : (const void*)dev::k_sample_t<false>;
     CUDA_TRY(raise_smem_limit(kfn, smem));
     int grid = 0;
