@@ -99,6 +99,10 @@ struct lda_trainer {
     std::vector<Slot> slots;
     std::vector<cudaEvent_t> ev_slot;
     cudaEvent_t ev_ready = nullptr;
+    // host-buffer sweeps: each chunk's topics are copied back on copy_stream as soon as the
+    // chunk is sampled
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_chunk = nullptr, ev_copied = nullptr;
     uint32_t *h_tok_doc = nullptr, *h_dtok_pos = nullptr, *h_dtok_word = nullptr;  // pinned [N]
     std::vector<int64_t> chunk_dt;  // [C+1] first doc-row entry of each chunk
     int64_t max_chunk_tok = 0, max_chunk_dt = 0, h2d_bytes = 0;
@@ -114,6 +118,12 @@ struct lda_trainer {
         }
         for (cudaEvent_t e : ev_slot) cudaEventDestroy(e);
         if (ev_ready) cudaEventDestroy(ev_ready);
+        if (copy_stream) {
+            cudaStreamSynchronize(copy_stream);
+            cudaStreamDestroy(copy_stream);
+        }
+        if (ev_chunk) cudaEventDestroy(ev_chunk);
+        if (ev_copied) cudaEventDestroy(ev_copied);
         cudaFreeHost(h_tok_doc);
         cudaFreeHost(h_dtok_pos);
         cudaFreeHost(h_dtok_word);
@@ -685,7 +695,18 @@ extern "C" int lda_trainer_sync(lda_trainer* t) {
     return finish(t);
 }
 
-static int sweep_async(lda_trainer* t, int ll_mode) {
+// Copies chunk ch's new topics to host buffer zout on the copy stream once the work
+// queued so far on stream q (the chunk's sampling) has finished.
+static int copy_back(lda_trainer* t, int ch, cudaStream_t q, uint16_t* zout) {
+    const int64_t t0 = t->chunk_tok[ch], n = t->chunk_tok[ch + 1] - t0;
+    if (n <= 0) return LDA_OK;
+    CUDA_TRY(cudaEventRecord(t->ev_chunk, q));
+    CUDA_TRY(cudaStreamWaitEvent(t->copy_stream, t->ev_chunk, 0));
+    CUDA_TRY(cudaMemcpyAsync(zout + t0, t->z + t0, sizeof(uint16_t) * (size_t)n, cudaMemcpyDeviceToHost, t->copy_stream));
+    return LDA_OK;
+}
+
+static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr) {
     int rc;
     if ((rc = lda_update_wt(t))) return rc;
     if ((rc = lda_max_topic(t))) return rc;
@@ -693,6 +714,7 @@ static int sweep_async(lda_trainer* t, int ll_mode) {
         for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
             if ((rc = lda_update_dt(t, ch))) return rc;
             if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
+            if (zout && (rc = copy_back(t, ch, t->stream, zout))) return rc;
         }
     } else {
         // chunk i of the range goes to slot / stream i mod S: its copy overlaps the
@@ -709,6 +731,7 @@ static int sweep_async(lda_trainer* t, int ll_mode) {
             if ((rc = load_chunk(t, ch, slot, q))) return rc;
             if ((rc = dt_launch(t, ch, slot, q))) return rc;
             if ((rc = sample_launch(t, ch, slot, ll_mode, q))) return rc;
+            if (zout && (rc = copy_back(t, ch, q, zout))) return rc;
         }
         for (int i = 0; i < S; ++i) {
             CUDA_TRY(cudaEventRecord(t->ev_slot[i], t->sstreams[i]));
@@ -745,11 +768,33 @@ extern "C" int lda_iterate_host(lda_trainer* t, const uint16_t* zin, uint16_t* z
     t->begin_stage(5);
     CUDA_TRY(cudaMemcpyAsync(t->z, zin, sizeof(uint16_t) * (size_t)t->N, cudaMemcpyHostToDevice, t->stream));
     t->end_stage();
-    int rc = sweep_async(t, ll_mode);
-    if (rc) return rc;
-    t->begin_stage(5);
-    CUDA_TRY(cudaMemcpyAsync(zout, t->z, sizeof(uint16_t) * (size_t)t->N, cudaMemcpyDeviceToHost, t->stream));
-    t->end_stage();
+    if (!t->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_chunk, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_copied, cudaEventDisableTiming));
+    }
+    // A pinned output buffer gets each chunk's topics as soon as the chunk is sampled; a
+    // device-to-host copy into pageable memory would block the host, so there the topics
+    // come back in one copy after the sweep.
+    cudaPointerAttributes pa{};
+    const bool pinned = cudaPointerGetAttributes(&pa, zout) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+    cudaGetLastError();
+    int rc;
+    if (pinned) {
+        // topics outside the sampled chunk range come back unchanged
+        const int64_t r0 = t->chunk_tok[t->chunk_first], r1 = t->chunk_tok[t->chunk_last];
+        if (r0 > 0) std::memcpy(zout, zin, sizeof(uint16_t) * (size_t)r0);
+        if (r1 < t->N) std::memcpy(zout + r1, zin + r1, sizeof(uint16_t) * (size_t)(t->N - r1));
+        if ((rc = sweep_async(t, ll_mode, zout))) return rc;
+        // the sweep is complete when the last chunk's copy has landed
+        CUDA_TRY(cudaEventRecord(t->ev_copied, t->copy_stream));
+        CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_copied, 0));
+    } else {
+        if ((rc = sweep_async(t, ll_mode))) return rc;
+        t->begin_stage(5);
+        CUDA_TRY(cudaMemcpyAsync(zout, t->z, sizeof(uint16_t) * (size_t)t->N, cudaMemcpyDeviceToHost, t->stream));
+        t->end_stage();
+    }
     if ((rc = finish(t))) return rc;
     if (ll_mode) {
         t->last_ll = *t->ll_host;

@@ -294,3 +294,29 @@ def test_trainers_of_different_k_coexist():
     big.iterate(2, ll=True)
     small.iterate(2, ll=True)
     big.iterate(1)
+
+
+@pytest.mark.parametrize("stream_mode,chunk_range", [(1, None), (1, (1, 3)), (2, None)])
+def test_host_iterate_pinned_buffers(stream_mode, chunk_range):
+    """With pinned host buffers each chunk's topics are copied back as soon as the chunk is
+    sampled (overlapping the later chunks); the result equals resident sweeps, and tokens
+    outside a sampled chunk range come back unchanged."""
+    import torch
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=4))
+    a = L.Trainer(c, K=64, stream_mode=1)
+    b = L.Trainer(c, K=64, stream_mode=stream_mode, num_streams=2)
+    if chunk_range:
+        a.set_chunk_range(*chunk_range)
+        b.set_chunk_range(*chunk_range)
+    z = c.topics()
+    zin = torch.empty(len(z), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    zout = torch.empty(len(z), dtype=torch.int16).pin_memory().numpy().view(np.uint16)
+    zin[:] = z
+    for it in range(3):
+        b.iterate_host(zin, zout)
+        a.iterate(1)
+        assert np.array_equal(a.topics(), zout), f"sweep {it}"
+        zin[:] = zout
+    if chunk_range:
+        t0, t1 = (int(x) for x in c.chunk_tok()[list(chunk_range)])
+        assert np.array_equal(zout[:t0], z[:t0]) and np.array_equal(zout[t1:], z[t1:])
