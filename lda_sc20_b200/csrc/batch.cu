@@ -106,15 +106,17 @@ __global__ void __launch_bounds__(256) kb_stats(BatchArgs b) {
 __global__ void __launch_bounds__(256) kb_dt(BatchArgs b) {
     extern __shared__ uint32_t smu[];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* hist = smu + (size_t)b.Kmax * wid;
-    for (int k = lane; k < b.Kmax; k += 32) hist[k] = 0u;
+    const int per = b.Kmax + dt_bit_words(b.Kmax);
+    uint32_t* hist = smu + (size_t)per * wid;
+    uint32_t* bits = hist + b.Kmax;
+    for (int k = lane; k < per; k += 32) hist[k] = 0u;
     __syncwarp();
     for (;;) {
         const int i = grab(b.counters + 2, lane);
         if (i >= b.n_dt) break;
         const uint4 u = b.dt_work[i];
         const DtArgs& a = b.dt[u.x];
-        for (uint32_t d = u.y; d < u.y + u.z; ++d) dt_doc(a, d, hist, lane);
+        for (uint32_t d = u.y; d < u.y + u.z; ++d) dt_doc(a, d, hist, bits, lane);
     }
 }
 
@@ -241,7 +243,7 @@ struct lda_batch {
     std::vector<double> ll_host;
     uint32_t host_sweeps = 0;
     // launch shapes
-    size_t smem_hist = 0, smem_stats = 0, smem_sample = 0;
+    size_t smem_hist = 0, smem_stats = 0, smem_sample = 0, smem_dt = 0;
     int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_sample_ll = 0;
     // cached graph of (sweeps, ll)
     cudaGraphExec_t graph = nullptr;
@@ -345,9 +347,10 @@ static int batch_build(lda_batch* b) {
     b->smem_hist = (size_t)tu.warps * b->Kmax * 4;
     b->smem_stats = (size_t)tu.warps * b->Kmax * 8;
     b->smem_sample = (size_t)tu.warps * ((b->Kmax + dev::col_words(b->Kmax)) * 4 + dev::C_NUM * 4);
+    b->smem_dt = (size_t)tu.warps * (b->Kmax + (b->Kmax + 31) / 32) * 4;
     if ((rc = occupancy((const void*)dev::kb_wt, threads, b->smem_hist, b->num_sms, &b->grid_wt)) ||
         (rc = occupancy((const void*)dev::kb_stats, threads, b->smem_stats, b->num_sms, &b->grid_stats)) ||
-        (rc = occupancy((const void*)dev::kb_dt, threads, b->smem_hist, b->num_sms, &b->grid_dt)) ||
+        (rc = occupancy((const void*)dev::kb_dt, threads, b->smem_dt, b->num_sms, &b->grid_dt)) ||
         (rc = occupancy((const void*)dev::kb_sample<false>, threads, b->smem_sample, b->num_sms, &b->grid_sample)) ||
         (rc = occupancy((const void*)dev::kb_sample<true>, threads, b->smem_sample, b->num_sms, &b->grid_sample_ll)))
         return rc;
@@ -386,7 +389,7 @@ static int enqueue_sweeps(lda_batch* b, int sweeps, int ll) {
         dev::kb_zero<<<std::min<int>((int)b->zero.n, 4 * b->num_sms), 256, 0, b->st>>>(b->zero.p, (int)b->zero.n, b->counters);
         dev::kb_wt<<<grid_for(b->grid_wt, a.n_wt, W), threads, b->smem_hist, b->st>>>(a);
         dev::kb_stats<<<grid_for(b->grid_stats, a.n_st, W), threads, b->smem_stats, b->st>>>(a);
-        dev::kb_dt<<<grid_for(b->grid_dt, a.n_dt, W), threads, b->smem_hist, b->st>>>(a);
+        dev::kb_dt<<<grid_for(b->grid_dt, a.n_dt, W), threads, b->smem_dt, b->st>>>(a);
         if (last_ll) dev::kb_sample<true><<<grid_for(b->grid_sample_ll, a.n_sm, W), threads, b->smem_sample, b->st>>>(a);
         else dev::kb_sample<false><<<grid_for(b->grid_sample, a.n_sm, W), threads, b->smem_sample, b->st>>>(a);
         if (last_ll) dev::kb_ll<<<M, 1024, 0, b->st>>>(b->sm.p, b->ll_dev);

@@ -54,11 +54,13 @@ __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
 __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
     extern __shared__ uint32_t smu[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* hist = smu + (size_t)a.K * wid;
-    for (int i = threadIdx.x; i < a.K * warps; i += blockDim.x) smu[i] = 0u;
+    const int per = a.K + dt_bit_words(a.K);
+    uint32_t* hist = smu + (size_t)per * wid;
+    uint32_t* bits = hist + a.K;
+    for (int i = threadIdx.x; i < per * warps; i += blockDim.x) smu[i] = 0u;
     __syncthreads();
     for (uint32_t d = a.d_begin + blockIdx.x * warps + wid; d < a.d_end; d += gridDim.x * warps) {
-        dt_doc(a, d, hist, lane);
+        dt_doc(a, d, hist, bits, lane);
     }
 }
 

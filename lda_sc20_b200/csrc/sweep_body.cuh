@@ -154,41 +154,84 @@ struct DtArgs {
     uint32_t tok_base, dt_base;
 };
 
-// Doc d: its counts in the warp's shared `hist` (zero on entry and on exit), the
-// per-token metadata and the compacted row.
-__device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hist, int lane) {
+// Doc d: its counts in the warp's shared `hist` (K words) and the bitmap of its non-zero
+// topics in `bits` (ceil(K/32) words), both zero on entry and on exit; the per-token
+// metadata; and the row, compacted from the bitmap: each lane takes 32 topics' bits, an
+// exclusive scan of their popcounts places its entries, ascending k.
+__device__ __forceinline__ int dt_bit_words(int K) { return (K + 31) >> 5; }
+
+__device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hist, uint32_t* bits, int lane) {
     const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
-    for (uint32_t base = 0; base < n; base += 32) {
-        bool valid = base + lane < n;
-        uint32_t k = valid ? (uint32_t)__ldg(a.z + __ldg(a.dtok_pos + (b - a.tok_base) + base + lane)) : 0xffffffffu;
-        if (valid && k >= (uint32_t)a.K) {
-            atomicOr(a.err, 1);
-            valid = false;
-            k = 0xfffffffeu;
+    const uint32_t* dpos = a.dtok_pos + (b - a.tok_base);
+    const uint32_t* dword = a.dtok_word + (b - a.tok_base);
+    // four 32-token steps per pass: their index loads, then their topic gathers, are in
+    // flight together
+    for (uint32_t base = 0; base < n; base += 128) {
+        uint32_t k[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t i = base + 32u * s + lane;
+            k[s] = i < n ? __ldg(dpos + i) : 0xffffffffu;
         }
-        const unsigned m = __match_any_sync(FULL, k);
-        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+#pragma unroll
+        for (int s = 0; s < 4; ++s) k[s] = k[s] != 0xffffffffu ? (uint32_t)__ldg(a.z + k[s]) : 0xffffffffu;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            bool valid = k[s] != 0xffffffffu;
+            uint32_t kk = k[s];
+            if (valid && kk >= (uint32_t)a.K) {
+                atomicOr(a.err, 1);
+                valid = false;
+                kk = 0xfffffffeu;
+            }
+            const unsigned m = __match_any_sync(FULL, kk);
+            if (valid && lane == __ffs(m) - 1) {
+                if (atomicAdd(&hist[kk], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
+            }
+        }
     }
     __syncwarp();
-    for (uint32_t i = lane; i < n; i += 32) {
-        const uint32_t pos = __ldg(a.dtok_pos + (b - a.tok_base) + i);
-        const uint32_t t2 = __ldg(a.st_top2 + __ldg(a.dtok_word + (b - a.tok_base) + i));
-        const uint32_t k1 = t2 & 0xffffu, k2 = t2 >> 16;
-        const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
-        a.meta[pos - a.tok_base] = (c2 << 16) | c1;
+    for (uint32_t base = 0; base < n; base += 128) {
+        uint32_t pos[4], t2[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t i = base + 32u * s + lane;
+            pos[s] = i < n ? __ldg(dpos + i) : 0xffffffffu;
+            t2[s] = i < n ? __ldg(dword + i) : 0u;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) t2[s] = pos[s] != 0xffffffffu ? __ldg(a.st_top2 + t2[s]) : 0u;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (pos[s] == 0xffffffffu) continue;
+            const uint32_t k1 = t2[s] & 0xffffu, k2 = t2[s] >> 16;
+            const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
+            a.meta[pos[s] - a.tok_base] = (c2 << 16) | c1;
+        }
     }
     __syncwarp();
     uint32_t* out = a.dt_ent + (__ldg(a.dt_off + d) - a.dt_base);
+    const int words = dt_bit_words(a.K);
     uint32_t nnz = 0;
-    for (int kb = 0; kb < a.K; kb += 32) {
-        const int k = kb + lane;
-        const uint32_t h = k < a.K ? hist[k] : 0u;
-        const unsigned bal = __ballot_sync(FULL, h != 0u);
-        if (h) {
-            out[nnz + __popc(bal & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+    for (int wb = 0; wb < words; wb += 32) {
+        const int wi = wb + lane;
+        uint32_t m = wi < words ? bits[wi] : 0u;
+        const uint32_t c = (uint32_t)__popc(m);
+        uint32_t incl = c;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t t = __shfl_up_sync(FULL, incl, off);
+            if (lane >= off) incl += t;
+        }
+        uint32_t p = nnz + incl - c;
+        nnz += __shfl_sync(FULL, incl, 31);
+        if (m) bits[wi] = 0u;
+        while (m) {
+            const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            out[p++] = (k << 16) | hist[k];
             hist[k] = 0u;
         }
-        nnz += (uint32_t)__popc(bal);
     }
     if (lane == 0) a.dt_nnz[d] = nnz;
     __syncwarp();

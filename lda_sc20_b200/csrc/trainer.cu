@@ -251,7 +251,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     if (sample_bytes(T.warps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
     T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
     T.smem_sample = sample_bytes(T.warps);
-    T.smem_dt = (size_t)T.warps * row;
+    T.smem_dt = (size_t)T.warps * (T.K + (T.K + 31) / 32) * 4;
 
     // ---- host-side derived layout
     const int64_t N = T.N, V = T.V, D = T.D, Vs = V - T.Vd;
