@@ -344,7 +344,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
         // per-lane record of this token's evaluation, for the deferred draw and counters
         const uint32_t* my_row = row;
         uint32_t my_b0 = 0, my_b1 = 0;
-        float my_t2 = 0.0f;
+        float my_t2 = 0.0f, my_total = 0.0f;
         int kind = BR_NONE;
         bool evaluated = false;
         const unsigned vmask = __ballot_sync(FULL, valid);
@@ -370,9 +370,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
             const float uj = __shfl_sync(FULL, u, j);
             const float pS = fadd(pmj, S);
             const float total = fadd(pS, Q);
-            if (LL) {
-                if (lane == j) ll += log((double)total / ((double)nd + a.den_add));
-            }
+            if (LL && lane == j) my_total = total;
             if (LL && ((emask >> j) & 1u)) continue;
             const float target = fmul(uj, total);
             if (target < pmj) {
@@ -413,6 +411,9 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
                 }
             }
         }
+        // each lane's own token's log-likelihood term, all lanes at once (every lane
+        // accumulates only its own tokens, in group order)
+        if (LL && valid) ll += log((double)my_total / ((double)nd + a.den_add));
         if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, col, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
