@@ -120,7 +120,7 @@ __global__ void __launch_bounds__(256) kb_dt(BatchArgs b) {
     }
 }
 
-template <bool LL>
+template <bool LL, int QB>
 __global__ void __launch_bounds__(256) kb_sample(BatchArgs b) {
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -147,7 +147,7 @@ __global__ void __launch_bounds__(256) kb_sample(BatchArgs b) {
             warp_recip(r, ca->n_k, ca->K, ca->Vbeta, lane);
         }
         const SampleArgs& a = *ca;
-        sample_tile<LL>(a, (int)w.y, a.tiles[w.y], a.iter + done, r, col, ctr, lane);
+        sample_tile<LL, QB>(a, (int)w.y, a.tiles[w.y], a.iter + done, r, col, ctr, lane);
     }
     __syncwarp();
     if (ca && lane < C_NUM && ctr[lane]) atomicAdd(ca->ctr + lane, (unsigned long long)ctr[lane]);
@@ -262,6 +262,12 @@ struct lda_batch {
     }
 };
 
+// Batched sampler instantiation: Q-bucket rounds four per batch when some model has K > 1024.
+static const void* batch_sample_kernel(bool ll, int Kmax) {
+    if (Kmax > 1024) return ll ? (const void*)dev::kb_sample<true, 4> : (const void*)dev::kb_sample<false, 4>;
+    return ll ? (const void*)dev::kb_sample<true, 1> : (const void*)dev::kb_sample<false, 1>;
+}
+
 static int occupancy(const void* fn, int threads, size_t smem, int num_sms, int* grid) {
     int per_sm = 0;
     CUDA_TRY(raise_smem_limit(fn, smem));
@@ -351,8 +357,8 @@ static int batch_build(lda_batch* b) {
     if ((rc = occupancy((const void*)dev::kb_wt, threads, b->smem_hist, b->num_sms, &b->grid_wt)) ||
         (rc = occupancy((const void*)dev::kb_stats, threads, b->smem_stats, b->num_sms, &b->grid_stats)) ||
         (rc = occupancy((const void*)dev::kb_dt, threads, b->smem_dt, b->num_sms, &b->grid_dt)) ||
-        (rc = occupancy((const void*)dev::kb_sample<false>, threads, b->smem_sample, b->num_sms, &b->grid_sample)) ||
-        (rc = occupancy((const void*)dev::kb_sample<true>, threads, b->smem_sample, b->num_sms, &b->grid_sample_ll)))
+        (rc = occupancy(batch_sample_kernel(false, b->Kmax), threads, b->smem_sample, b->num_sms, &b->grid_sample)) ||
+        (rc = occupancy(batch_sample_kernel(true, b->Kmax), threads, b->smem_sample, b->num_sms, &b->grid_sample_ll)))
         return rc;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
@@ -390,8 +396,14 @@ static int enqueue_sweeps(lda_batch* b, int sweeps, int ll) {
         dev::kb_wt<<<grid_for(b->grid_wt, a.n_wt, W), threads, b->smem_hist, b->st>>>(a);
         dev::kb_stats<<<grid_for(b->grid_stats, a.n_st, W), threads, b->smem_stats, b->st>>>(a);
         dev::kb_dt<<<grid_for(b->grid_dt, a.n_dt, W), threads, b->smem_dt, b->st>>>(a);
-        if (last_ll) dev::kb_sample<true><<<grid_for(b->grid_sample_ll, a.n_sm, W), threads, b->smem_sample, b->st>>>(a);
-        else dev::kb_sample<false><<<grid_for(b->grid_sample, a.n_sm, W), threads, b->smem_sample, b->st>>>(a);
+        const int gs = last_ll ? grid_for(b->grid_sample_ll, a.n_sm, W) : grid_for(b->grid_sample, a.n_sm, W);
+        if (b->Kmax > 1024) {
+            if (last_ll) dev::kb_sample<true, 4><<<gs, threads, b->smem_sample, b->st>>>(a);
+            else dev::kb_sample<false, 4><<<gs, threads, b->smem_sample, b->st>>>(a);
+        } else {
+            if (last_ll) dev::kb_sample<true, 1><<<gs, threads, b->smem_sample, b->st>>>(a);
+            else dev::kb_sample<false, 1><<<gs, threads, b->smem_sample, b->st>>>(a);
+        }
         if (last_ll) dev::kb_ll<<<M, 1024, 0, b->st>>>(b->sm.p, b->ll_dev);
         dev::kb_advance<<<1, 1, 0, b->st>>>(b->sweeps_done);
         CUDA_TRY(cudaGetLastError());

@@ -143,6 +143,52 @@ __device__ __forceinline__ int warp_level2(uint32_t n, float t2, int fallback, i
     return last >= 0 ? last : fallback;
 }
 
+// warp_level2 with QB rounds loaded and scanned together: the rounds' terms and their
+// Kogge-Stone scans are independent, only the carry links them, so QB scans run
+// interleaved and the rounds are then decided in order with the same additions
+// (carry + the round's total equals the round's last prefix).  QB = 1 is warp_level2.
+template <int QB, class Slot>
+__device__ __forceinline__ int warp_level2_rounds(uint32_t n, float t2, int fallback, int lane, Slot slot) {
+    if (QB == 1) return warp_level2(n, t2, fallback, lane, slot);
+    float carry = 0.0f;
+    int last = -1;
+    for (uint32_t base = 0; base < n; base += 32u * QB) {
+        float ks[QB];
+        int key[QB];
+        bool ok[QB];
+#pragma unroll
+        for (int q = 0; q < QB; ++q) {
+            key[q] = -1;
+            ks[q] = 0.0f;
+            ok[q] = false;
+            const uint32_t i = base + 32u * q + lane;
+            if (i < n) slot(i, key[q], ks[q], ok[q]);
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int q = 0; q < QB; ++q) {
+                const float t = __shfl_up_sync(FULL, ks[q], off);
+                if (lane >= off) ks[q] = fadd(ks[q], t);
+            }
+        }
+        float tot[QB];
+#pragma unroll
+        for (int q = 0; q < QB; ++q) tot[q] = __shfl_sync(FULL, ks[q], 31);
+#pragma unroll
+        for (int q = 0; q < QB; ++q) {
+            if (base + 32u * q >= n) break;
+            const float P = fadd(carry, ks[q]);
+            const unsigned f = __ballot_sync(FULL, ok[q] && t2 < P);
+            const unsigned v = __ballot_sync(FULL, ok[q]);
+            if (f) return __shfl_sync(FULL, key[q], __ffs(f) - 1);
+            if (v) last = __shfl_sync(FULL, key[q], 31 - __clz(v));
+            carry = fadd(carry, tot[q]);
+        }
+    }
+    return last >= 0 ? last : fallback;
+}
+
 // Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
 // loads of two entries are issued together); col in the sampler's skewed layout.
 __device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,

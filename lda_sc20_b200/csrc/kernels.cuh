@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
 }
 
 // Sampler: warp per tile, tiles taken from an atomic counter.
-template <bool LL>
+template <bool LL, int QB = 1>
 __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleArgs a) {
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleA
         tile = __shfl_sync(FULL, tile, 0);
         if (tile >= a.ntiles) break;
         const int4 t = a.tiles[tile];
-        sample_tile<LL>(a, tile, t, a.iter, r, col, ctr, lane);
+        sample_tile<LL, QB>(a, tile, t, a.iter, r, col, ctr, lane);
     }
     __syncwarp();
     if (lane < C_NUM && ctr[lane]) atomicAdd(a.ctr + lane, (unsigned long long)ctr[lane]);

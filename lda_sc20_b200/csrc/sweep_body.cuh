@@ -297,8 +297,9 @@ enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 
 // One sampler tile (tile index `tile` of a.tiles, content t) with the word column in the
 // warp's shared `col` (col_words(K) floats, skewed layout), the reciprocal table `r` and
-// the warp's shared counter row `ctr`.
-template <bool LL>
+// the warp's shared counter row `ctr`.  QB: Q-bucket rounds decided per batch (1 for
+// K <= 1024, where a lane has one round of topics).
+template <bool LL, int QB = 1>
 __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
                                             const float* r, float* col, uint32_t* ctr, int lane) {
     const int w = t.x;
@@ -398,7 +399,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
                 const int K = a.K;
                 const float alpha = a.alpha;
                 const uint32_t n = (uint32_t)((K - ls + 31) / 32);
-                const int zq = warp_level2(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                const int zq = warp_level2_rounds<QB>(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
                     const int k = ls + 32 * (int)i;
                     const float cz = col[col_skew(k)];
                     key = k;

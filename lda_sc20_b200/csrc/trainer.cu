@@ -203,6 +203,25 @@ static int occupancy_grid(const void* fn, int threads, size_t smem, int num_sms,
     return LDA_OK;
 }
 
+// The sampler instantiation for (LL mode, K): for K > 1024 a lane's Q-bucket topics span
+// several rounds, which are decided four per batch.
+static int sample_qb(int K) { return K > 1024 ? 4 : 1; }
+
+static const void* sample_kernel(bool ll, int K) {
+    if (sample_qb(K) == 4) return ll ? (const void*)dev::k_sample_t<true, 4> : (const void*)dev::k_sample_t<false, 4>;
+    return ll ? (const void*)dev::k_sample_t<true, 1> : (const void*)dev::k_sample_t<false, 1>;
+}
+
+static void launch_sample(bool ll, int K, int grid, int threads, size_t smem, cudaStream_t q, const dev::SampleArgs& a) {
+    if (sample_qb(K) == 4) {
+        if (ll) dev::k_sample_t<true, 4><<<grid, threads, smem, q>>>(a);
+        else dev::k_sample_t<false, 4><<<grid, threads, smem, q>>>(a);
+    } else {
+        if (ll) dev::k_sample_t<true, 1><<<grid, threads, smem, q>>>(a);
+        else dev::k_sample_t<false, 1><<<grid, threads, smem, q>>>(a);
+    }
+}
+
 extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* cfg, lda_trainer** out) {
     if (!c || !cfg || !out) return fail(LDA_ERR_ARG, "null argument");
     *out = nullptr;
@@ -409,15 +428,15 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     // ---- launch shapes: persistent grids sized by occupancy
     const int threads = 32 * T.warps;
     for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
-                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair((const void*)dev::k_sample_t<false>, T.smem_sample),
-                    std::make_pair((const void*)dev::k_sample_t<true>, T.smem_sample)})
+                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair(sample_kernel(false, T.K), T.smem_sample),
+                    std::make_pair(sample_kernel(true, T.K), T.smem_sample)})
         CUDA_TRY(raise_smem_limit(kv.first, kv.second));
     if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
-    if ((rc = occupancy_grid((const void*)dev::k_sample_t<false>, threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+    if ((rc = occupancy_grid(sample_kernel(false, T.K), threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
     int grid_ll = 0;
-    if ((rc = occupancy_grid((const void*)dev::k_sample_t<true>, threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
+    if ((rc = occupancy_grid(sample_kernel(true, T.K), threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
     T.grid_sample = std::min(T.grid_sample, grid_ll);
     T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
     CUDA_TRY(cudaDeviceSynchronize());
@@ -607,8 +626,7 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
     CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(unsigned), q));
     if (n > 0) {
         const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
-        if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * t->warps, t->smem_sample, q>>>(a);
-        else dev::k_sample_t<false><<<grid, 32 * t->warps, t->smem_sample, q>>>(a);
+        launch_sample(a.ll_mode != 0, t->K, grid, 32 * t->warps, t->smem_sample, q, a);
         CUDA_TRY(cudaGetLastError());
     }
     t->chunk_sampled_ll[chunk] = ll_mode != 0;
@@ -1148,7 +1166,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
     const size_t smem = (size_t)io->K * 4 + (size_t)warps * (dev::col_words(io->K) * 4 + 16 * sizeof(uint32_t));
     if (warps < 1 || smem > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
-    const void* kfn = io->ll_mode ? (const void*)dev::k_sample_t<true> : (const void*)dev::k_sample_t<false>;
+    const void* kfn = sample_kernel(io->ll_mode != 0, io->K);
     CUDA_TRY(raise_smem_limit(kfn, smem));
     int grid = 0;
     if ((rc = occupancy_grid(kfn, 32 * warps, smem, num_sms, &grid))) return rc;
@@ -1170,8 +1188,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
     a.tok_base = 0;
     a.dt_base = 0;
-    if (a.ll_mode) dev::k_sample_t<true><<<grid, 32 * warps, smem, st>>>(a);
-    else dev::k_sample_t<false><<<grid, 32 * warps, smem, st>>>(a);
+    launch_sample(a.ll_mode != 0, io->K, grid, 32 * warps, smem, st, a);
     CUDA_TRY(cudaGetLastError());
     if (io->ll_mode) {
         dev::k_ll_reduce<<<1, 1024, 0, st>>>(a.tile_ll, io->num_tiles, io->ll_sum);
