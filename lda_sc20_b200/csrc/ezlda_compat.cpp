@@ -2,7 +2,7 @@
 //
 //   ezlda_compat <chunk_dir> [--K 1024] [--alpha 50/K] [--beta 0.01] [--iters 100]
 //                [--seed 42] [--device 0] [--ll-every 1] [--record FILE]
-//                [--checkpoint FILE] [--resume FILE]
+//                [--checkpoint FILE] [--resume FILE] [--budget-gb G] [--streams S]
 //
 // Reads the EZLDA chunk directory (lengthVec.txt, docLength.txt, TLLength.txt, TLSplit.txt,
 // chunk<c>/...), runs the sweeps on one GPU through the C ABI and prints per sweep
@@ -12,6 +12,8 @@
 // (EZLDA/utility.cu:2143); the value is the FP64 log-likelihood of profilePerp
 // (profilePerp/utility.cu:2398,2810) instead of EZLDA's token counter.  Per-sweep
 // times go to the record file like EZLDA's SamplingDRecord.txt (mainKernel.cu:376).
+// Like EZLDA, chunks stream through the device when the corpus exceeds --budget-gb (or
+// always with --streams S > 0, on S CUDA streams); otherwise the corpus stays resident.
 // Unlike EZLDA (exit() on any error), errors print the library's message and return 1.
 #include <chrono>
 #include <cstdio>
@@ -29,12 +31,13 @@ static int die(const char* what) {
 int main(int argc, char** argv) {
     if (argc < 2 || std::strcmp(argv[1], "--help") == 0) {
         std::fprintf(stderr, "usage: %s <chunk_dir> [--K n] [--alpha a] [--beta b] [--iters n] [--seed s] "
-                             "[--device d] [--ll-every n] [--record file] [--checkpoint file] [--resume file]\n", argv[0]);
+                             "[--device d] [--ll-every n] [--record file] [--checkpoint file] [--resume file] "
+                             "[--budget-gb g] [--streams s]\n", argv[0]);
         return 2;
     }
     const char* dir = argv[1];
-    int K = 1024, iters = 100, device = 0, ll_every = 1;
-    double alpha = -1.0, beta = 0.01;
+    int K = 1024, iters = 100, device = 0, ll_every = 1, streams = 0;
+    double alpha = -1.0, beta = 0.01, budget_gb = 0.0;
     unsigned long long seed = 42;
     std::string record = "SamplingDRecord.txt", ckpt, resume;
     for (int i = 2; i < argc; ++i) {
@@ -53,6 +56,8 @@ int main(int argc, char** argv) {
         else if (a == "--record") record = next();
         else if (a == "--checkpoint") ckpt = next();
         else if (a == "--resume") resume = next();
+        else if (a == "--budget-gb") budget_gb = std::atof(next());
+        else if (a == "--streams") streams = std::atoi(next());
         else { std::fprintf(stderr, "unknown option %s\n", a.c_str()); return 2; }
     }
     if (alpha <= 0) alpha = 50.0 / K;  // EZLDA/Argument.cuh:9
@@ -68,7 +73,9 @@ int main(int argc, char** argv) {
     cfg.beta = (float)beta;
     cfg.seed = seed;
     cfg.device = device;
-    cfg.device_budget = 0;
+    cfg.device_budget = (int64_t)(budget_gb * 1073741824.0);
+    cfg.stream_mode = streams > 0 ? 2 : 0;
+    cfg.num_streams = streams;
     lda_trainer* tr = nullptr;
     if (lda_trainer_create(corpus, &cfg, &tr) != LDA_OK) return die("creating the trainer");
     lda_corpus_free(corpus);
@@ -76,6 +83,9 @@ int main(int argc, char** argv) {
     int64_t bytes = 0;
     lda_trainer_device_bytes(tr, &bytes);
     std::printf("Total memory usage : %f GB\n", bytes / 1e9);
+    int32_t streaming = 0, nstreams = 0;
+    lda_trainer_stream_info(tr, &streaming, &nstreams, nullptr);
+    if (streaming) std::printf("chunks streamed through %d CUDA streams\n", nstreams);
     FILE* rec = record.empty() ? nullptr : std::fopen(record.c_str(), "w");
     uint32_t it0 = 0;
     lda_trainer_get_iteration(tr, &it0);

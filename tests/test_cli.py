@@ -41,3 +41,21 @@ def test_cli_runs_sweeps_and_prints_ll(tmp_path):
     t2 = L.Trainer(L.Corpus.load_ezlda(d), K=64)
     t2.restore(ck)
     assert t2.iteration == 3 and np.array_equal(t2.topics(), t.topics())
+
+
+@pytest.mark.gpu
+def test_cli_streams_chunks(tmp_path):
+    """--streams streams the chunks (EZLDA's mode of operation) with the same LL line."""
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=3))
+    d = str(tmp_path / "chunks")
+    c.write_ezlda(d, 64)
+    out = []
+    for extra in ([], ["--streams", "2"]):
+        r = subprocess.run([CLI, d, "--K", "64", "--iters", "2", "--record", ""] + extra,
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        out.append([float(x) for x in re.findall(r"^iter \d+ loglik (\S+)", r.stdout, re.M)])
+        if extra:
+            assert "chunks streamed through 2 CUDA streams" in r.stdout
+    assert out[0] == out[1]
+
