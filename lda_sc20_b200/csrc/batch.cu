@@ -428,6 +428,8 @@ extern "C" int lda_batch_create(lda_trainer* const* trainers, int32_t n, const l
         for (int j = 0; j < m; ++j)
             if (trainers[j] == trainers[m]) return fail(LDA_ERR_ARG, "trainer %d appears twice", m);
         b->Kmax = std::max(b->Kmax, b->views[m].K);
+        if (b->views[m].K > dev::kLargeK)
+            return fail(LDA_ERR_ARG, "trainer %d has K=%d; batched models take K <= %d", m, b->views[m].K, dev::kLargeK);
     }
     b->device = b->views[0].device;
     if (tuning) b->tuning = *tuning;

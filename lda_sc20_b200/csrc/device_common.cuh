@@ -189,20 +189,29 @@ __device__ __forceinline__ int warp_level2_rounds(uint32_t n, float t2, int fall
     return last >= 0 ? last : fallback;
 }
 
+// The sampler's view of the tile's word column: colz(k) = phi_k of the word with its max
+// topic zeroed.  ColShared reads a column built in shared memory (skewed layout, with the
+// max topic's slot already zeroed).
+struct ColShared {
+    const float* col;
+    __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
+};
+
 // Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
-// loads of two entries are issued together); col in the sampler's skewed layout.
+// loads of two entries are issued together).
+template <class View>
 __device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
-                                            const float* col) {
+                                            const View& colz) {
     float acc = 0.0f;
     uint32_t q = b0;
     for (; q + 2 <= b1; q += 2) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 1);
-        acc = ffma(u2f(e0 & 0xffffu), col[col_skew((int)(e0 >> 16))], acc);
-        acc = ffma(u2f(e1 & 0xffffu), col[col_skew((int)(e1 >> 16))], acc);
+        acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
+        acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
     }
     if (q < b1) {
         const uint32_t e = __ldg(row + q);
-        acc = ffma(u2f(e & 0xffffu), col[col_skew((int)(e >> 16))], acc);
+        acc = ffma(u2f(e & 0xffffu), colz((int)(e >> 16)), acc);
     }
     return acc;
 }
@@ -210,14 +219,15 @@ __device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, ui
 // The S-bucket draw inside one lane block: the block's serial partial sums (the same
 // fmaf chain as block_mass) are compared with t2; the first entry with colz > 0 whose
 // partial sum exceeds t2 wins, else the last entry with colz > 0, else `fallback`.
+template <class View>
 __device__ __forceinline__ int block_draw(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
-                                          const float* col, float t2, int fallback) {
+                                          const View& colz, float t2, int fallback) {
     float acc = 0.0f;
     int last = -1;
     for (uint32_t q = b0; q < b1; ++q) {
         const uint32_t e = __ldg(row + q);
         const int k = (int)(e >> 16);
-        const float cz = col[col_skew(k)];
+        const float cz = colz(k);
         acc = ffma(u2f(e & 0xffffu), cz, acc);
         if (cz > 0.0f) {
             last = k;

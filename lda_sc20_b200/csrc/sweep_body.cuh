@@ -284,6 +284,10 @@ struct SampleArgs {
     uint32_t tok_base, dt_base;
 };
 
+// Above this many topics the trainer samples with the CTA-per-tile dense-word kernel and
+// the column-free sparse-word kernel (kernels.cuh) instead of a column per warp.
+constexpr int kLargeK = 2048;
+
 // Sweep counters live in shared memory (one row per warp, written by lane 0) so they
 // cost no registers in the sampling loop.
 enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE, C_ROWS, C_RENT, C_NUM };
@@ -295,34 +299,18 @@ enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE,
 // Branch taken by a token (counters only).
 enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 
-// One sampler tile (tile index `tile` of a.tiles, content t) with the word column in the
-// warp's shared `col` (col_words(K) floats, skewed layout), the reciprocal table `r` and
-// the warp's shared counter row `ctr`.  QB: Q-bucket rounds decided per batch (1 for
-// K <= 1024, where a lane has one round of topics).
-template <bool LL, int QB = 1>
-__device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
-                                            const float* r, float* col, uint32_t* ctr, int lane) {
-    const int w = t.x;
-    const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
-    __syncwarp();
-    uint32_t wnnz = 0;
-    build_column<true>(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
-    if (lane == 0) {
-        ctr[C_WNNZ] += wnnz;
-        ctr[w < a.Vd ? C_TDENSE : C_TSPARSE] += 1u;
-    }
-    const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
-    const float4 ph = __ldg(a.st_phi + w);
-    const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
-    const float QP = warp_ks_scan(QL, lane);
-    const float Q = __shfl_sync(FULL, QP, 31);
-    if (lane == 0) col[col_skew(maxK)] = 0.0f;
-    __syncwarp();
+// The 32-token groups g0, g0 + gstep, ... of the token range [start, start + cnt) of one
+// word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word).
+// Returns the lane's LL partial (LL mode).
+template <bool LL, int QB, class View>
+__device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t start, uint32_t cnt, uint32_t g0,
+                                                uint32_t gstep, uint32_t iter, int maxK, const float4 ph, float QL,
+                                                float QP, float Q, const View& colz, uint32_t* ctr, int lane) {
     double ll = 0.0;
     uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
     const uint32_t* row = a.dt_ent;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
-    for (uint32_t g = 0; g < cnt; g += 32) {
+    for (uint32_t g = g0; g < cnt; g += gstep) {
         const bool valid = g + lane < cnt;
         const uint32_t tok = start + g + lane;
         uint32_t d = 0xffffffffu, nd = 0, my_nnz = 0, my_off = 0;
@@ -362,7 +350,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
                 row = a.dt_ent + __shfl_sync(FULL, my_off, j);
                 B = (nnz + 31u) >> 5;
                 const uint32_t b0 = min(lane * B, nnz);
-                SL = block_mass(row, b0, min(b0 + B, nnz), col);
+                SL = block_mass(row, b0, min(b0 + B, nnz), colz);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
                 evaluated |= (lane == j);
@@ -401,7 +389,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
                 const uint32_t n = (uint32_t)((K - ls + 31) / 32);
                 const int zq = warp_level2_rounds<QB>(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
                     const int k = ls + 32 * (int)i;
-                    const float cz = col[col_skew(k)];
+                    const float cz = colz(k);
                     key = k;
                     term = fmul(alpha, cz);
                     ok = cz > 0.0f;
@@ -415,7 +403,7 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
         // each lane's own token's log-likelihood term, all lanes at once (every lane
         // accumulates only its own tokens, in group order)
         if (LL && valid) ll += log((double)my_total / ((double)nd + a.den_add));
-        if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, col, my_t2, maxK);
+        if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, colz, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
         const bool in_need = (need0 >> lane) & 1u;
@@ -435,6 +423,33 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
             ctr[C_RENT] += nnz_rows;
         }
     }
+    return ll;
+}
+
+// One sampler tile (tile index `tile` of a.tiles, content t) with the word column in the
+// warp's shared `col` (col_words(K) floats, skewed layout), the reciprocal table `r` and
+// the warp's shared counter row `ctr`.  QB: Q-bucket rounds decided per batch (1 for
+// K <= 1024, where a lane has one round of topics).
+template <bool LL, int QB = 1>
+__device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
+                                            const float* r, float* col, uint32_t* ctr, int lane) {
+    const int w = t.x;
+    const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
+    __syncwarp();
+    uint32_t wnnz = 0;
+    build_column<true>(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, &wnnz);
+    if (lane == 0) {
+        ctr[C_WNNZ] += wnnz;
+        ctr[w < a.Vd ? C_TDENSE : C_TSPARSE] += 1u;
+    }
+    const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
+    const float4 ph = __ldg(a.st_phi + w);
+    const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
+    const float QP = warp_ks_scan(QL, lane);
+    const float Q = __shfl_sync(FULL, QP, 31);
+    if (lane == 0) col[col_skew(maxK)] = 0.0f;
+    __syncwarp();
+    double ll = sample_groups<LL, QB>(a, start, cnt, 0u, 32u, iter, maxK, ph, QL, QP, Q, ColShared{col}, ctr, lane);
     if (LL) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);

@@ -28,6 +28,8 @@ namespace {
 #define LDA_SAMPLE_TILE 512
 #endif
 constexpr int kSampleTile = LDA_SAMPLE_TILE;  // tokens per sampler tile (a word's column is rebuilt per tile)
+constexpr int kDenseTileLarge = 2048;         // dense-word tiles above kLargeK topics (one CTA per tile)
+constexpr int kLargeWarps = 8;                // warps per CTA of the large-K sampler kernels
 constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
 constexpr int kCounters = 16;
 
@@ -48,6 +50,10 @@ struct lda_trainer {
     int64_t N = 0, V = 0, D = 0;
     std::vector<int64_t> chunk_tok, chunk_doc;
     std::vector<int> s_tile_base;  // [C+1]
+    // K > kLargeK: a chunk's sampler tiles are its dense-word tiles, then its sparse-word
+    // tiles from s_tile_split[chunk] on, each kind sampled by its own kernel
+    bool large = false;
+    std::vector<int> s_tile_split;  // [C]
     int n_wtiles = 0;
 
     // device arrays
@@ -63,14 +69,14 @@ struct lda_trainer {
     uint32_t *seg_off = nullptr, *seg_cnt = nullptr;
     int4 *s_tiles = nullptr, *w_tiles = nullptr;
     double *tile_ll = nullptr, *ll_dev = nullptr;
-    unsigned* tile_ctr = nullptr;         // [1 + C]
+    unsigned* tile_ctr = nullptr;         // [1 + 2C]: word-topic tiles, then per chunk sampler tiles (two kinds)
     unsigned long long* ctr = nullptr;    // [kCounters]
     int* err = nullptr;
     double* ll_host = nullptr;            // pinned
 
     int64_t dt_cap = 0, swt_cap = 0;
-    size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0;
-    int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0;
+    size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0, smem_dense = 0, smem_sparse = 0;
+    int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_dense = 0, grid_sparse = 0;
 
     std::vector<void*> allocs;
     int64_t bytes = 0, budget = 0;
@@ -212,6 +218,15 @@ static const void* sample_kernel(bool ll, int K) {
     return ll ? (const void*)dev::k_sample_t<true, 1> : (const void*)dev::k_sample_t<false, 1>;
 }
 
+// K > kLargeK: the dense-word (CTA per tile) and sparse-word (no column) samplers; a lane's
+// Q-bucket topics span more than one round there, so four rounds are decided per batch.
+static const void* dense_large_kernel(bool ll) {
+    return ll ? (const void*)dev::k_sample_dense_large<true, 4> : (const void*)dev::k_sample_dense_large<false, 4>;
+}
+static const void* sparse_large_kernel(bool ll) {
+    return ll ? (const void*)dev::k_sample_sparse_large<true, 4> : (const void*)dev::k_sample_sparse_large<false, 4>;
+}
+
 static void launch_sample(bool ll, int K, int grid, int threads, size_t smem, cudaStream_t q, const dev::SampleArgs& a) {
     if (sample_qb(K) == 4) {
         if (ll) dev::k_sample_t<true, 4><<<grid, threads, smem, q>>>(a);
@@ -266,10 +281,19 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     T.warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (T.warps < 1) return fail(LDA_ERR_ARG, "K=%d needs %lld bytes of shared memory per warp (max %d)", T.K, (long long)(2 * row), max_smem);
     auto sample_bytes = [&](int w) { return (size_t)T.K * 4 + (size_t)w * (dev::col_words(T.K) * 4 + 16 * sizeof(uint32_t)); };
-    while (T.warps > 1 && sample_bytes(T.warps) > (size_t)max_smem) --T.warps;
-    if (sample_bytes(T.warps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
+    T.large = T.K > dev::kLargeK;
+    if (!T.large) {
+        while (T.warps > 1 && sample_bytes(T.warps) > (size_t)max_smem) --T.warps;
+        if (sample_bytes(T.warps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
+        T.smem_sample = sample_bytes(T.warps);
+    } else {
+        T.smem_dense = dev::dense_large_smem(T.K, kLargeWarps);
+        T.smem_sparse = dev::sparse_large_smem(T.K, kLargeWarps);
+        if (T.smem_dense > (size_t)max_smem || T.smem_sparse > (size_t)max_smem)
+            return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory (the dense-word sampler needs %zu bytes)", T.K,
+                        T.smem_dense);
+    }
     T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
-    T.smem_sample = sample_bytes(T.warps);
     T.smem_dt = (size_t)T.warps * (T.K + (T.K + 31) / 32) * 4;
 
     // ---- host-side derived layout
@@ -293,18 +317,28 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         run += std::min<int64_t>(c->word_count[T.Vd + s], T.K);
     }
     T.swt_cap = run;
-    // sampler tiles per chunk, largest first
+    // sampler tiles per chunk, largest first (for K > kLargeK: dense-word tiles, then
+    // sparse-word tiles, each largest first)
     std::vector<int4> st;
     T.s_tile_base.assign(T.C + 1, 0);
+    T.s_tile_split.assign(T.C, 0);
+    auto by_size = [](const int4& a, const int4& b) { return a.z > b.z; };
     for (int ch = 0; ch < T.C; ++ch) {
-        std::vector<int4> ct;
+        std::vector<int4> ct, cs;
         for (int64_t w = 0; w < V; ++w) {
             const int64_t n = c->seg_cnt[(size_t)ch * V + w], o = c->seg_off[(size_t)ch * V + w];
-            for (int64_t p = 0; p < n; p += kSampleTile)
-                ct.push_back(make_int4((int)w, (int)(o + p), (int)std::min<int64_t>(kSampleTile, n - p), w < T.Vd));
+            const bool dense = w < T.Vd;
+            const int64_t tile = T.large && dense ? kDenseTileLarge : kSampleTile;
+            for (int64_t p = 0; p < n; p += tile) {
+                const int4 v = make_int4((int)w, (int)(o + p), (int)std::min<int64_t>(tile, n - p), dense);
+                (T.large && !dense ? cs : ct).push_back(v);
+            }
         }
-        std::stable_sort(ct.begin(), ct.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
+        std::stable_sort(ct.begin(), ct.end(), by_size);
+        std::stable_sort(cs.begin(), cs.end(), by_size);
         st.insert(st.end(), ct.begin(), ct.end());
+        T.s_tile_split[ch] = (int)st.size();
+        st.insert(st.end(), cs.begin(), cs.end());
         T.s_tile_base[ch + 1] = (int)st.size();
     }
     // word-topic tiles: dense segments of every chunk, and one tile per sparse word
@@ -342,7 +376,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
-                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + T.C, 4) + nb(kCounters, 8) +
+                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + 2 * T.C, 4) + nb(kCounters, 8) +
                                  nb(1, 4);
         T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
     }
@@ -386,7 +420,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.seg_off, (int64_t)T.C * V); ALLOC(T.seg_cnt, (int64_t)T.C * V);
     ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
-    ALLOC(T.tile_ctr, 1 + T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
+    ALLOC(T.tile_ctr, 1 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
 
@@ -428,16 +462,32 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     // ---- launch shapes: persistent grids sized by occupancy
     const int threads = 32 * T.warps;
     for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
-                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt), std::make_pair(sample_kernel(false, T.K), T.smem_sample),
-                    std::make_pair(sample_kernel(true, T.K), T.smem_sample)})
+                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt)})
         CUDA_TRY(raise_smem_limit(kv.first, kv.second));
     if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
-    if ((rc = occupancy_grid(sample_kernel(false, T.K), threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
-    int grid_ll = 0;
-    if ((rc = occupancy_grid(sample_kernel(true, T.K), threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
-    T.grid_sample = std::min(T.grid_sample, grid_ll);
+    if (!T.large) {
+        int grid_ll = 0;
+        for (bool ll : {false, true}) CUDA_TRY(raise_smem_limit(sample_kernel(ll, T.K), T.smem_sample));
+        if ((rc = occupancy_grid(sample_kernel(false, T.K), threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+        if ((rc = occupancy_grid(sample_kernel(true, T.K), threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
+        T.grid_sample = std::min(T.grid_sample, grid_ll);
+    } else {
+        const int lt = 32 * kLargeWarps;
+        int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
+        for (bool ll : {false, true}) {
+            CUDA_TRY(raise_smem_limit(dense_large_kernel(ll), T.smem_dense));
+            CUDA_TRY(raise_smem_limit(sparse_large_kernel(ll), T.smem_sparse));
+        }
+        if ((rc = occupancy_grid(dense_large_kernel(false), lt, T.smem_dense, T.num_sms, &g0)) ||
+            (rc = occupancy_grid(dense_large_kernel(true), lt, T.smem_dense, T.num_sms, &g1)) ||
+            (rc = occupancy_grid(sparse_large_kernel(false), lt, T.smem_sparse, T.num_sms, &g2)) ||
+            (rc = occupancy_grid(sparse_large_kernel(true), lt, T.smem_sparse, T.num_sms, &g3)))
+            return rc;
+        T.grid_dense = std::min(g0, g1);
+        T.grid_sparse = std::min(g2, g3);
+    }
     T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
     CUDA_TRY(cudaDeviceSynchronize());
     T.chunk_sampled_ll.assign(T.C, false);
@@ -623,6 +673,33 @@ static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, in
 static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaStream_t q) {
     const dev::SampleArgs a = sample_args(t, chunk, slot, ll_mode);
     const int n = a.ntiles;
+    if (t->large) {
+        // dense-word tiles [base, split): one CTA each; sparse-word tiles [split, end)
+        const int nd = t->s_tile_split[chunk] - t->s_tile_base[chunk], ns = n - nd;
+        dev::SampleArgs ad = a, as = a;
+        ad.ntiles = nd;
+        as.tiles += nd;
+        as.tile_ll += nd;
+        as.ntiles = ns;
+        as.tile_counter = t->tile_ctr + 1 + t->C + chunk;
+        CUDA_TRY(cudaMemsetAsync(ad.tile_counter, 0, sizeof(unsigned), q));
+        CUDA_TRY(cudaMemsetAsync(as.tile_counter, 0, sizeof(unsigned), q));
+        const bool ll = ll_mode != 0;
+        if (nd > 0) {
+            const int grid = std::max(1, std::min(t->grid_dense, nd));
+            if (ll) dev::k_sample_dense_large<true, 4><<<grid, 32 * kLargeWarps, t->smem_dense, q>>>(ad);
+            else dev::k_sample_dense_large<false, 4><<<grid, 32 * kLargeWarps, t->smem_dense, q>>>(ad);
+            CUDA_TRY(cudaGetLastError());
+        }
+        if (ns > 0) {
+            const int grid = std::max(1, std::min(t->grid_sparse, (ns + kLargeWarps - 1) / kLargeWarps));
+            if (ll) dev::k_sample_sparse_large<true, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, q>>>(as);
+            else dev::k_sample_sparse_large<false, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, q>>>(as);
+            CUDA_TRY(cudaGetLastError());
+        }
+        t->chunk_sampled_ll[chunk] = ll;
+        return LDA_OK;
+    }
     CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(unsigned), q));
     if (n > 0) {
         const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));

@@ -101,10 +101,12 @@ def test_k_variants(K):
     c = L.Corpus.generate(L.corpus_config("c0", num_docs=500, vocab=800, K=K, num_chunks=2))
     tr, o = _setup(c, K)
     z = c.topics()
-    for it in range(3):
-        o.iterate(z, 7, it, ll=True)
     tr2 = L.Trainer(c, K=K, seed=7)
-    tr2.iterate(3, ll=True)
+    for it in range(3):
+        st = o.iterate(z, 7, it, ll=True)
+        tr2.iterate(1, ll=True)
+        s, _ = tr2.loglik()
+        assert abs(s - st.loglik) <= LL_RTOL * abs(st.loglik), f"LL at sweep {it}"
     assert np.array_equal(tr2.topics(), z)
     del tr
 
@@ -237,12 +239,12 @@ def test_config1_full_size_properties():
     assert tr2.loglik()[0] == ll
 
 
-@pytest.mark.parametrize("streams", [1, 2, 3])
-def test_streamed_chunks_equal_resident(streams):
+@pytest.mark.parametrize("streams,K", [(1, 64), (2, 64), (3, 64), (2, 4096)])
+def test_streamed_chunks_equal_resident(streams, K):
     """Chunks streamed through `streams` slot buffers (EZLDA/mainKernel.cu:203-314) give the
-    same topics, LL and counters as the resident corpus, sweep after sweep."""
-    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=5, dense_kind=1, dense_param=0.05))
-    K = 64
+    same topics, LL and counters as the resident corpus, sweep after sweep (K=4096: the
+    dense-word and sparse-word samplers of large K)."""
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=5, dense_kind=1, dense_param=0.05, K=K))
     res = L.Trainer(c, K=K, seed=42, stream_mode=1)
     stm = L.Trainer(c, K=K, seed=42, stream_mode=2, num_streams=streams)
     assert res.stream_info()[0] is False
