@@ -65,15 +65,17 @@ __global__ void kb_zero(const ZeroSeg* segs, int nseg, unsigned* counters) {
 __global__ void __launch_bounds__(256) kb_wt(BatchArgs b) {
     extern __shared__ uint32_t smu[];
     const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    uint32_t* hist = smu + (size_t)b.Kmax * wid;
-    for (int k = lane; k < b.Kmax; k += 32) hist[k] = 0u;
+    const int per = b.Kmax + wt_bit_words(b.Kmax);
+    uint32_t* hist = smu + (size_t)per * wid;
+    uint32_t* bits = hist + b.Kmax;
+    for (int k = lane; k < per; k += 32) hist[k] = 0u;
     __syncwarp();
     for (;;) {
         const int i = grab(b.counters + 0, lane);
         if (i >= b.n_wt) break;
         const uint2 w = b.wt_work[i];
         const WtArgs& a = b.wt[w.x];
-        wt_tile(a, a.tiles[w.y], hist, reinterpret_cast<unsigned*>(a.n_k), lane);
+        wt_tile(a, a.tiles[w.y], hist, bits, reinterpret_cast<unsigned*>(a.n_k), lane);
     }
 }
 
@@ -350,7 +352,7 @@ static int batch_build(lda_batch* b) {
         return rc;
     // launch shapes
     const int threads = 32 * tu.warps;
-    b->smem_hist = (size_t)tu.warps * b->Kmax * 4;
+    b->smem_hist = (size_t)tu.warps * (b->Kmax + (b->Kmax + 31) / 32) * 4;
     b->smem_stats = (size_t)tu.warps * b->Kmax * 8;
     b->smem_sample = (size_t)tu.warps * ((b->Kmax + dev::col_words(b->Kmax)) * 4 + dev::C_NUM * 4);
     b->smem_dt = (size_t)tu.warps * (b->Kmax + (b->Kmax + 31) / 32) * 4;

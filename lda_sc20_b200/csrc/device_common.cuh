@@ -55,8 +55,10 @@ __device__ __forceinline__ float token_uniform(uint32_t seed_lo, uint32_t seed_h
     return u2f(x >> 8) * 0x1p-24f;
 }
 
+// Histogram of topics z[start, start + cnt) into the warp's shared `hist`; a topic whose
+// count leaves zero also gets its bit in `bits` (ceil(K/32) words).
 __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uint32_t start, uint32_t cnt,
-                                             uint32_t* hist, int K, int lane, int* err) {
+                                             uint32_t* hist, uint32_t* bits, int K, int lane, int* err) {
     for (uint32_t base = 0; base < cnt; base += 32) {
         const uint32_t i = base + lane;
         bool valid = i < cnt;
@@ -67,7 +69,9 @@ __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uin
             k = 0xfffffffeu;
         }
         const unsigned m = __match_any_sync(FULL, k);
-        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k], (uint32_t)__popc(m));
+        if (valid && lane == __ffs(m) - 1) {
+            if (atomicAdd(&hist[k], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[k >> 5], 1u << (k & 31u));
+        }
     }
 }
 

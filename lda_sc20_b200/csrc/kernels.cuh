@@ -18,9 +18,11 @@ namespace dev {
 __global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
     extern __shared__ uint32_t smu[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int per = a.K + wt_bit_words(a.K);
     uint32_t* nk = smu;
-    uint32_t* hist = smu + (size_t)a.K * (1 + wid);
-    for (int i = threadIdx.x; i < a.K * (warps + 1); i += blockDim.x) smu[i] = 0u;
+    uint32_t* hist = smu + a.K + (size_t)per * wid;
+    uint32_t* bits = hist + a.K;
+    for (int i = threadIdx.x; i < a.K + per * warps; i += blockDim.x) smu[i] = 0u;
     __syncthreads();
     for (;;) {
         int tile = 0;
@@ -28,7 +30,7 @@ __global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
         tile = __shfl_sync(FULL, tile, 0);
         if (tile >= a.ntiles) break;
         const int4 t = a.tiles[tile];
-        wt_tile(a, t, hist, nk, lane);
+        wt_tile(a, t, hist, bits, nk, lane);
     }
     __syncthreads();
     for (int k = threadIdx.x; k < a.K; k += blockDim.x) {

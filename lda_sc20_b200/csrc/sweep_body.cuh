@@ -39,25 +39,35 @@ struct WtArgs {
     int* err;
 };
 
-// One word tile: histogram its topics in the warp's shared row `hist` (zero on entry and
-// on exit) and add it to the dense row or write the sparse row; topic totals go to `nk`
-// (a CTA-private shared array, or the model's global totals).
-__device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t* hist, unsigned* nk, int lane) {
+// One word tile: histogram its topics in the warp's shared row `hist` (K words) with the
+// bitmap of its non-zero topics in `bits` (ceil(K/32) words), both zero on entry and on
+// exit, and add it to the dense row or write the sparse row (ascending k, placed by a
+// prefix scan of the bitmap words' popcounts); topic totals go to `nk` (a CTA-private
+// shared array, or the model's global totals).
+__device__ __forceinline__ int wt_bit_words(int K) { return (K + 31) >> 5; }
+
+__device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t* hist, uint32_t* bits, unsigned* nk,
+                                        int lane) {
     const int w = t.x;
     if (t.w & 1) {
-        hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, a.K, lane, a.err);
+        hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, bits, a.K, lane, a.err);
     } else {
         for (int c = 0; c < a.C; ++c) {
             const size_t idx = (size_t)c * a.V + w;
-            hist_segment(a.z, a.seg_off[idx], a.seg_cnt[idx], hist, a.K, lane, a.err);
+            hist_segment(a.z, a.seg_off[idx], a.seg_cnt[idx], hist, bits, a.K, lane, a.err);
         }
     }
     __syncwarp();
+    const int words = wt_bit_words(a.K);
     if (t.w & 1) {
         int* row = a.dwt + (size_t)w * a.K;
-        for (int k = lane; k < a.K; k += 32) {
-            const uint32_t h = hist[k];
-            if (h) {
+        for (int wi = lane; wi < words; wi += 32) {
+            uint32_t m = bits[wi];
+            if (m) bits[wi] = 0u;
+            while (m) {
+                const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+                m &= m - 1u;
+                const uint32_t h = hist[k];
                 atomicAdd(row + k, (int)h);
                 atomicAdd(nk + k, h);
                 hist[k] = 0u;
@@ -67,16 +77,27 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t*
         const int s = w - a.Vd;
         uint32_t* out = a.swt_ent + a.swt_off[s];
         uint32_t nnz = 0;
-        for (int kb = 0; kb < a.K; kb += 32) {
-            const int k = kb + lane;
-            const uint32_t h = k < a.K ? hist[k] : 0u;
-            const unsigned b = __ballot_sync(FULL, h != 0u);
-            if (h) {
-                out[nnz + __popc(b & ((1u << lane) - 1u))] = ((uint32_t)k << 16) | h;
+        for (int wb = 0; wb < words; wb += 32) {
+            const int wi = wb + lane;
+            uint32_t m = wi < words ? bits[wi] : 0u;
+            const uint32_t c = (uint32_t)__popc(m);
+            uint32_t incl = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, incl, off);
+                if (lane >= off) incl += v;
+            }
+            uint32_t p = nnz + incl - c;
+            nnz += __shfl_sync(FULL, incl, 31);
+            if (m) bits[wi] = 0u;
+            while (m) {
+                const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+                m &= m - 1u;
+                const uint32_t h = hist[k];
+                out[p++] = (k << 16) | h;
                 atomicAdd(nk + k, h);
                 hist[k] = 0u;
             }
-            nnz += (uint32_t)__popc(b);
         }
         if (lane == 0) a.swt_nnz[s] = nnz;
     }
@@ -104,18 +125,40 @@ struct StatsArgs {
 // Statistics of word w from its column (built into the warp's shared `col`).
 __device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const float* r, float* col, int lane) {
     build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, nullptr);
-    float v1 = -1.0f;
-    int k1 = 0x7fffffff;
-    for (int k = lane; k < a.K; k += 32) if (col[k] > v1) { v1 = col[k]; k1 = k; }
-    warp_argmax(v1, k1);
-    float v2 = -1.0f;
-    int k2 = 0x7fffffff;
-    for (int k = lane; k < a.K; k += 32) if (k != k1 && col[k] > v2) { v2 = col[k]; k2 = k; }
-    warp_argmax(v2, k2);
-    float v3 = -1.0f;
-    int k3 = 0x7fffffff;
-    for (int k = lane; k < a.K; k += 32) if (k != k1 && k != k2 && col[k] > v3) { v3 = col[k]; k3 = k; }
-    warp_argmax(v3, k3);
+    // the lane's top three by (phi desc, k asc) in one pass (k ascends, so a strictly larger
+    // value is needed to displace), then three warp-wide pops of the lanes' heads
+    float a1 = -1.0f, a2 = -1.0f, a3 = -1.0f;
+    int i1 = 0x7fffffff, i2 = 0x7fffffff, i3 = 0x7fffffff;
+    for (int k = lane; k < a.K; k += 32) {
+        const float x = col[k];
+        if (x > a1) {
+            a3 = a2; i3 = i2;
+            a2 = a1; i2 = i1;
+            a1 = x; i1 = k;
+        } else if (x > a2) {
+            a3 = a2; i3 = i2;
+            a2 = x; i2 = k;
+        } else if (x > a3) {
+            a3 = x; i3 = k;
+        }
+    }
+    float v[3];
+    int kk[3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r) {
+        float bv = a1;
+        int bk = i1;
+        warp_argmax(bv, bk);
+        v[r] = bv;
+        kk[r] = bk;
+        if (i1 == bk) {
+            a1 = a2; i1 = i2;
+            a2 = a3; i2 = i3;
+            a3 = -1.0f; i3 = 0x7fffffff;
+        }
+    }
+    const float v1 = v[0], v2 = v[1], v3 = v[2];
+    const int k1 = kk[0], k2 = kk[1], k3 = kk[2];
     float ql = 0.0f;
     for (int k = lane; k < a.K; k += 32) if (k != k1) ql = ffma(a.alpha, col[k], ql);
     const float qp = warp_ks_scan(ql, lane);

@@ -293,7 +293,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory (the dense-word sampler needs %zu bytes)", T.K,
                         T.smem_dense);
     }
-    T.smem_wt = T.smem_stats = (size_t)(T.warps + 1) * row;
+    auto wt_bytes = [&](int w) { return ((size_t)T.K + (size_t)w * (T.K + (T.K + 31) / 32)) * 4; };
+    while (T.warps > 1 && wt_bytes(T.warps) > (size_t)max_smem) --T.warps;
+    T.smem_stats = (size_t)(T.warps + 1) * row;
+    T.smem_wt = wt_bytes(T.warps);
     T.smem_dt = (size_t)T.warps * (T.K + (T.K + 31) / 32) * 4;
 
     // ---- host-side derived layout
