@@ -127,12 +127,15 @@ __host__ __device__ __forceinline__ size_t sparse_large_smem(int K, int warps) {
     return (size_t)K * 4 + (size_t)warps * (large_bit_words(K) * 4 + large_pre_words(K) * 2 + C_NUM * 4);
 }
 
-// Shared memory of the dense-word kernel: r[K], the shared column, the warps' counter rows
-// and their LL partials.
+// Shared memory of the dense-word kernel: the shared column, the warps' counter rows and
+// their LL partials (the reciprocals are formed while the column is built).
 __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
-    return (((size_t)K * 4 + (size_t)col_words(K) * 4 + (size_t)warps * C_NUM * 4 + 7) & ~(size_t)7) +
-           (size_t)warps * 8;
+    return (((size_t)col_words(K) * 4 + (size_t)warps * C_NUM * 4 + 7) & ~(size_t)7) + (size_t)warps * 8;
 }
+
+#ifndef LDA_DENSE_LARGE_MIN_BLOCKS
+#define LDA_DENSE_LARGE_MIN_BLOCKS 4
+#endif
 
 template <bool LL, int QB>
 __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_sparse_large(SampleArgs a) {
@@ -206,17 +209,15 @@ __global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_sparse_la
 }
 
 template <bool LL, int QB>
-__global__ void __launch_bounds__(256, 2) k_sample_dense_large(SampleArgs a) {
+__global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dense_large(SampleArgs a) {
     extern __shared__ float smf[];
     __shared__ int s_tile;
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float* r = smf;
-    float* col = smf + a.K;
+    float* col = smf;
     uint32_t* ctr_all = reinterpret_cast<uint32_t*>(col + col_words(a.K));
     uint32_t* ctr = ctr_all + C_NUM * wid;
     double* wll = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(ctr_all + C_NUM * warps) + 7) & ~(uintptr_t)7);
-    fill_recip(r, a.n_k, a.K, a.Vbeta);
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();
     for (;;) {
@@ -227,8 +228,12 @@ __global__ void __launch_bounds__(256, 2) k_sample_dense_large(SampleArgs a) {
         const int4 t = a.tiles[tile];
         const int w = t.x;
         const int* wrow = a.dwt + (size_t)w * a.K;
-        for (int k = threadIdx.x; k < a.K; k += blockDim.x)
-            col[col_skew(k)] = fmul(fadd(__int2float_rn(__ldg(wrow + k)), a.beta), r[k]);
+        // phi_k = ((float)n_wk + beta) * r_k with r_k = 1 / ((float)n_k + V*beta), the values
+        // fill_recip and build_column form
+        for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+            const float rk = __fdiv_rn(1.0f, fadd(__int2float_rn(__ldg(a.n_k + k)), a.Vbeta));
+            col[col_skew(k)] = fmul(fadd(__int2float_rn(__ldg(wrow + k)), a.beta), rk);
+        }
         const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
         __syncthreads();
         if (threadIdx.x == 0) {
