@@ -334,7 +334,6 @@ def run_ours(args, world, rank, local):
     tr.set_topics(z0)                            # time sweeps 0..K-1 of a fresh run
     tr.iteration = 0
     tr.reset_stats()
-    tr.set_timing(True)
     barrier()
     torch.cuda.synchronize()
     e0 = torch.cuda.Event(enable_timing=True)
@@ -347,9 +346,18 @@ def run_ours(args, world, rank, local):
     clk = clocks.stop()
     ms_local = e0.elapsed_time(e1)
     ms = reduce_max(ms_local)
+    # the same sweeps again with per-stage CUDA events (stages run one at a time on the
+    # trainer's stream then), for the stage split and the sampler's roofline
+    tr.set_topics(z0)
+    tr.iteration = 0
+    tr.reset_stats()
+    tr.set_timing(True)
+    tr.iterate(args.steps, ll=False)
+    torch.cuda.synchronize()
     tm = tr.timing()
     cnt = tr.counters()
     tr.set_timing(False)
+    ms_staged = tm.ms_wt + tm.ms_stats + tm.ms_dt + tm.ms_sample
     # log-likelihood of the state after the K timed sweeps (one extra evaluation sweep)
     z_after = tr.topics()
     ll_mean = tr.iterate(1, ll=True)
@@ -443,8 +451,12 @@ def run_ours(args, world, rank, local):
                          "ms_per_launch": ms_per_launch},
             "stages_ms_per_sweep": {"wt": tm.ms_wt / sweeps, "stats": tm.ms_stats / sweeps,
                                     "dt": tm.ms_dt / sweeps, "sample": tm.ms_sample / sweeps,
+                                    "sum_staged": ms_staged / sweeps,
                                     "note": ("streamed: 'sample' spans copies, doc-row rebuilds and sampling "
-                                             "of all chunks on their streams") if streaming else ""},
+                                             "of all chunks on their streams") if streaming else
+                                            ("stages timed one at a time in a second pass over the same sweeps; "
+                                             "the timed run overlaps one chunk's doc-topic rebuild and sampling "
+                                             "with the next chunk's")},
             "sweep_ms_trace": trace,
             "sweep_counters": {"early_accept_frac": cnt.early_accept / max(cnt.tokens, 1),
                                "mean_nnz_full": cnt.sum_nnz_full / max(cnt.full, 1),

@@ -204,6 +204,10 @@ int lda_trainer_set_topics(lda_trainer* t, const uint16_t* in, int64_t count);
 int lda_trainer_get_iteration(const lda_trainer* t, uint32_t* iter);
 int lda_trainer_set_iteration(lda_trainer* t, uint32_t iter);
 int lda_trainer_counters(lda_trainer* t, lda_sweep_counters* out);
+/* Per-stage CUDA-event timing.  While it is on, a resident trainer runs its chunks'
+ * doc-topic rebuilds and sampling one at a time on its stream; while it is off, chunk i of
+ * the range runs on work stream i mod 2, overlapping the next chunk's work with this one's
+ * (the results are the same either way). */
 int lda_trainer_set_timing(lda_trainer* t, int32_t enabled);
 int lda_trainer_timing(lda_trainer* t, lda_stage_timing* out);
 int lda_trainer_reset_stats(lda_trainer* t);

@@ -109,6 +109,10 @@ struct lda_trainer {
     // chunk is sampled
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_chunk = nullptr, ev_copied = nullptr;
+    // resident sweeps without stage timing run chunk i of the range on work stream i mod 2,
+    // so one chunk's doc-topic rebuild and sampling overlap the other's
+    cudaStream_t work[2] = {nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
     uint32_t *h_tok_doc = nullptr, *h_dtok_pos = nullptr, *h_dtok_word = nullptr;  // pinned [N]
     std::vector<int64_t> chunk_dt;  // [C+1] first doc-row entry of each chunk
     int64_t max_chunk_tok = 0, max_chunk_dt = 0, h2d_bytes = 0;
@@ -130,6 +134,14 @@ struct lda_trainer {
         }
         if (ev_chunk) cudaEventDestroy(ev_chunk);
         if (ev_copied) cudaEventDestroy(ev_copied);
+        for (int i = 0; i < 2; ++i) {
+            if (work[i]) {
+                cudaStreamSynchronize(work[i]);
+                cudaStreamDestroy(work[i]);
+            }
+            if (ev_join[i]) cudaEventDestroy(ev_join[i]);
+        }
+        if (ev_fork) cudaEventDestroy(ev_fork);
         cudaFreeHost(h_tok_doc);
         cudaFreeHost(h_dtok_pos);
         cudaFreeHost(h_dtok_word);
@@ -808,11 +820,36 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr) {
     int rc;
     if ((rc = lda_update_wt(t))) return rc;
     if ((rc = lda_max_topic(t))) return rc;
-    if (!t->streaming) {
+    if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2)) {
+        // one stream, so that the stage events time each stage alone
         for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
             if ((rc = lda_update_dt(t, ch))) return rc;
             if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
             if (zout && (rc = copy_back(t, ch, t->stream, zout))) return rc;
+        }
+    } else if (!t->streaming) {
+        // chunk i of the range on work stream i mod 2: the next chunk's doc-topic rebuild
+        // fills the tail of this chunk's sampling, and the samplings' tails overlap.  Chunks
+        // are independent within a sweep (each reads and writes only its own tokens' topics
+        // and doc rows).
+        if (!t->work[0]) {
+            for (int i = 0; i < 2; ++i) {
+                CUDA_TRY(cudaStreamCreateWithFlags(&t->work[i], cudaStreamNonBlocking));
+                CUDA_TRY(cudaEventCreateWithFlags(&t->ev_join[i], cudaEventDisableTiming));
+            }
+            CUDA_TRY(cudaEventCreateWithFlags(&t->ev_fork, cudaEventDisableTiming));
+        }
+        CUDA_TRY(cudaEventRecord(t->ev_fork, t->stream));
+        for (int i = 0; i < 2; ++i) CUDA_TRY(cudaStreamWaitEvent(t->work[i], t->ev_fork, 0));
+        for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
+            cudaStream_t q = t->work[(ch - t->chunk_first) & 1];
+            if ((rc = dt_launch(t, ch, 0, q))) return rc;
+            if ((rc = sample_launch(t, ch, 0, ll_mode, q))) return rc;
+            if (zout && (rc = copy_back(t, ch, q, zout))) return rc;
+        }
+        for (int i = 0; i < 2; ++i) {
+            CUDA_TRY(cudaEventRecord(t->ev_join[i], t->work[i]));
+            CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_join[i], 0));
         }
     } else {
         // chunk i of the range goes to slot / stream i mod S: its copy overlaps the
