@@ -47,6 +47,8 @@ ALPHA = {"c2": 0.1}  # other presets: 50/K
 
 def workload(preset: str) -> str:
     return WORKLOADS.get(preset, f"corpus preset {preset}")
+
+
 HBM_FALLBACK_GBS = 6650.0
 
 
