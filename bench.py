@@ -42,7 +42,7 @@ WORKLOADS = {
            "words, 8 chunks; sweeps 0..K-1 from random initial topics"),
 }
 WORKLOAD = WORKLOADS["c1"]
-ALPHA = {"c2": 0.1}  # other presets: 50/K
+ALPHA = {"c2": 0.1, "c2s": 0.1}  # other presets: 50/K
 
 
 def workload(preset: str) -> str:

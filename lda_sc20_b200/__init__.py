@@ -61,6 +61,9 @@ def corpus_config(name: str, **over) -> GenConfig:
                          len_p2=0.0, len_min=1, len_max=2000, phi_kind=2, phi_conc=0.05, phi_zipf_s=1.05,
                          theta_conc=0.1, K=10000, dense_kind=2, dense_param=20000.0, num_chunks=8,
                          corpus_seed=1002, topic_seed=42)
+    # c2 at one tenth of the documents and a fifth of the vocabulary (~25M tokens), for
+    # profiler captures of the large-K kernels
+    presets["c2s"] = dict(presets["c2"], num_docs=100000, vocab=200000, dense_param=4000.0)
     if name not in presets:
         raise KeyError(f"unknown corpus preset {name!r} (have {sorted(presets)})")
     d = dict(presets[name])
