@@ -56,21 +56,31 @@ __device__ __forceinline__ float token_uniform(uint32_t seed_lo, uint32_t seed_h
 }
 
 // Histogram of topics z[start, start + cnt) into the warp's shared `hist`; a topic whose
-// count leaves zero also gets its bit in `bits` (ceil(K/32) words).
+// count leaves zero also gets its bit in `bits` (ceil(K/32) words).  Four 32-token steps
+// of topic loads are in flight together.
 __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uint32_t start, uint32_t cnt,
                                              uint32_t* hist, uint32_t* bits, int K, int lane, int* err) {
-    for (uint32_t base = 0; base < cnt; base += 32) {
-        const uint32_t i = base + lane;
-        bool valid = i < cnt;
-        uint32_t k = valid ? (uint32_t)__ldg(z + start + i) : 0xffffffffu;
-        if (valid && k >= (uint32_t)K) {
-            atomicOr(err, 1);
-            valid = false;
-            k = 0xfffffffeu;
+    for (uint32_t base = 0; base < cnt; base += 128) {
+        uint32_t k[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t i = base + 32u * s + lane;
+            k[s] = i < cnt ? (uint32_t)__ldg(z + start + i) : 0xffffffffu;
         }
-        const unsigned m = __match_any_sync(FULL, k);
-        if (valid && lane == __ffs(m) - 1) {
-            if (atomicAdd(&hist[k], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[k >> 5], 1u << (k & 31u));
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (base + 32u * s >= cnt) break;
+            bool valid = k[s] != 0xffffffffu;
+            uint32_t kk = k[s];
+            if (valid && kk >= (uint32_t)K) {
+                atomicOr(err, 1);
+                valid = false;
+                kk = 0xfffffffeu;
+            }
+            const unsigned m = __match_any_sync(FULL, kk);
+            if (valid && lane == __ffs(m) - 1) {
+                if (atomicAdd(&hist[kk], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
+            }
         }
     }
 }

@@ -52,9 +52,20 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t*
     if (t.w & 1) {
         hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, bits, a.K, lane, a.err);
     } else {
-        for (int c = 0; c < a.C; ++c) {
-            const size_t idx = (size_t)c * a.V + w;
-            hist_segment(a.z, a.seg_off[idx], a.seg_cnt[idx], hist, bits, a.K, lane, a.err);
+        // a sparse word's segments in every chunk: lane c loads chunk c's offset and count
+        for (int c0 = 0; c0 < a.C; c0 += 32) {
+            const int c = c0 + lane;
+            uint32_t so = 0, sc = 0;
+            if (c < a.C) {
+                const size_t idx = (size_t)c * a.V + w;
+                so = __ldg(a.seg_off + idx);
+                sc = __ldg(a.seg_cnt + idx);
+            }
+            const int nc = min(32, a.C - c0);
+            for (int j = 0; j < nc; ++j) {
+                const uint32_t o = __shfl_sync(FULL, so, j), n = __shfl_sync(FULL, sc, j);
+                if (n) hist_segment(a.z, o, n, hist, bits, a.K, lane, a.err);
+            }
         }
     }
     __syncwarp();
