@@ -649,7 +649,7 @@ def run_batch(args, local):
     import numpy as np
     import torch
     import lda_sc20_b200 as L
-    from lda_sc20_b200.batch import Batch, batch_corpus_configs
+    from lda_sc20_b200.batch import Batch, batch_corpus_configs, dense_words_for, tune_dense_rule
 
     torch.cuda.set_device(local)
     cfgs = batch_corpus_configs(args.batch_models)
@@ -669,9 +669,13 @@ def run_batch(args, local):
     t0 = time.perf_counter()
     ll_plain = [t.iterate(sweeps, ll=True) for t in plain]
     plain_s = time.perf_counter() - t0
-    batched = [L.Trainer(c, K=K, seed=11 + i, device=local) for i, (c, K) in enumerate(zip(corpora, Ks))]
-    b = Batch(batched)
+    # layout: the dense-word rule, picked on a sample of the models; then the batch's
+    # launch tuning on the whole batch
     t0 = time.perf_counter()
+    rule, rule_ms = tune_dense_rule(corpora, Ks, [11 + i for i in range(len(corpora))], device=local)
+    batched = [L.Trainer(c, K=K, seed=11 + i, device=local, num_dense=dense_words_for(c, K, rule))
+               for i, (c, K) in enumerate(zip(corpora, Ks))]
+    b = Batch(batched)
     tuning, tuned_ms = b.autotune(sweeps_per_trial=2)
     tune_s = time.perf_counter() - t0
     l0, _ = b.stats()
@@ -691,7 +695,10 @@ def run_batch(args, local):
             "batched_vs_plain": plain_s / batch_s,
             "seconds": {"plain_sequential": plain_s, "batched": batch_s, "autotune": tune_s},
             "autotune": {"warps": tuning[0], "schedule": ["largest_first", "model_major"][tuning[1]],
-                         "tile_tokens": tuning[2], "ms_per_sweep": tuned_ms},
+                         "tile_tokens": tuning[2], "ms_per_sweep": tuned_ms,
+                         "dense_rule": {"None": "corpus split (count >= K)", "-1": "no dense words"}.get(
+                             str(rule), f"count >= {rule}*K"),
+                         "dense_rule_ms_per_sweep_on_sample": {str(k): round(v[0], 3) for k, v in rule_ms.items()}},
             "gpu_launches": l1 - l0, "work_items_per_sweep": work,
             "models_identical_to_plain": f"{same}/{len(corpora)}", "loglik_max_rel_diff": ll_rel,
             "clocks": clk}

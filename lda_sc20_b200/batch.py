@@ -87,3 +87,40 @@ def batch_corpus_configs(n: int, seed: int = 3):
         out.append(corpus_config("c0", num_docs=D, vocab=V, gen_topics=16, len_p1=80.0, len_min=1, len_max=400,
                                  K=K, num_chunks=1, corpus_seed=100000 + 7919 * m + seed, topic_seed=42 + m))
     return out
+
+
+def dense_words_for(corpus, K: int, rule):
+    """The trainer's num_dense for a dense-word rule: None keeps the corpus' split, -1 makes
+    no word dense, and a float f makes the words with at least f*K tokens dense (words are
+    frequency ranks; words above 65535 tokens are dense under every rule)."""
+    if rule is None:
+        return 0
+    wc = corpus.word_count()
+    forced = int((wc > 65535).sum())
+    if rule == -1:
+        return forced if forced else -1
+    n = max(int((wc >= rule * K).sum()), forced)
+    return n if n else -1
+
+
+def tune_dense_rule(corpora, Ks, seeds, rules=(None, -1, 0.5, 1.0, 4.0), sample: int = 64,
+                    sweeps_per_trial: int = 2, device: int = 0, rng_seed: int = 0):
+    """Picks the dense-word rule for a batch: on a random sample of the models, builds a
+    batch per rule, lets the batch autotuner pick its best tuning, and keeps the rule
+    whose best sweep is fastest.  The rule changes only the layout, never a result.
+    Returns (rule, {rule: (ms per sweep, tuning)})."""
+    from . import Trainer
+    rng = np.random.default_rng(rng_seed)
+    idx = rng.choice(len(corpora), size=min(sample, len(corpora)), replace=False)
+    timings = {}
+    for rule in rules:
+        trs = [Trainer(corpora[i], K=Ks[i], seed=seeds[i], device=device,
+                       num_dense=dense_words_for(corpora[i], Ks[i], rule)) for i in idx]
+        b = Batch(trs)
+        tuning, ms = b.autotune(sweeps_per_trial=sweeps_per_trial)
+        timings[rule] = (ms, tuning)
+        b.close()
+        for t in trs:
+            t.close()
+    best = min(timings, key=lambda r: timings[r][0])
+    return best, timings

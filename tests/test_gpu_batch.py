@@ -78,3 +78,26 @@ def test_batch_refuses_foreign_sweeps_and_streaming():
         Batch([st])
     with pytest.raises(L.LdaError):
         Batch([tr[0], tr[0]])
+
+
+def test_dense_rule_tuner_and_rules_change_no_result():
+    """The layout tuner picks one of its rules from timings on a sample; a batch built
+    under any rule gives the plain trainers' topics."""
+    from lda_sc20_b200.batch import dense_words_for, tune_dense_rule
+    models = _models(6, seed=9, scale=0.3)
+    corpora = [c for c, _ in models]
+    Ks = [K for _, K in models]
+    seeds = [11 + i for i in range(len(models))]
+    rules = (None, -1, 0.5, 4.0)
+    best, timings = tune_dense_rule(corpora, Ks, seeds, rules=rules, sample=4, sweeps_per_trial=1)
+    assert best in rules and set(timings) == set(rules) and all(v[0] > 0 for v in timings.values())
+    plain = _trainers(models)
+    for t in plain:
+        t.iterate(3)
+    for rule in rules:
+        trs = [L.Trainer(c, K=K, seed=11 + i, num_dense=dense_words_for(c, K, rule))
+               for i, (c, K) in enumerate(models)]
+        b = Batch(trs)
+        b.iterate(3)
+        for i, t in enumerate(plain):
+            assert np.array_equal(t.topics(), trs[i].topics()), f"rule {rule}, model {i}"
