@@ -263,6 +263,169 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
     if (lane < C_NUM && ctr[lane]) atomicAdd(a.ctr + lane, (unsigned long long)ctr[lane]);
 }
 
+// ------------------------------------------------------------ large-K word statistics
+// For K > kLargeK a sparse word's column is beta * r_k except at its own few topics, so its
+// statistics need no column: the top three come from its own topics and the first three
+// other topics of the CTA's list of topics in decreasing beta * r_k (ties to the lower k),
+// and the Q partials from one pass forming each phi_k as build_column does.  Dense words
+// keep k_word_stats.
+constexpr int kOrderList = 64;
+
+// (v, k) ranks above (a, i): larger value, ties to the lower topic.
+__device__ __forceinline__ bool ranks_above(float v, int k, float a, int i) { return v > a || (v == a && k < i); }
+
+__device__ __forceinline__ void top3_insert(float v, int k, float& a1, int& i1, float& a2, int& i2, float& a3, int& i3) {
+    if (ranks_above(v, k, a1, i1)) {
+        a3 = a2; i3 = i2;
+        a2 = a1; i2 = i1;
+        a1 = v; i1 = k;
+    } else if (ranks_above(v, k, a2, i2)) {
+        a3 = a2; i3 = i2;
+        a2 = v; i2 = k;
+    } else if (ranks_above(v, k, a3, i3)) {
+        a3 = v; i3 = k;
+    }
+}
+
+__host__ __device__ __forceinline__ size_t stats_sparse_smem(int K, int warps) {
+    return (size_t)K * 4 + kOrderList * 4 + (size_t)warps * (large_bit_words(K) * 4 + large_pre_words(K) * 2);
+}
+
+__global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
+    extern __shared__ float smf[];
+    __shared__ float red_v[8];
+    __shared__ int red_k[8];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bw = large_bit_words(a.K), pw = large_pre_words(a.K);
+    float* r = smf;
+    int* order = reinterpret_cast<int*>(smf + a.K);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * wid;
+    uint16_t* pre = reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * warps) +
+                    (size_t)pw * wid;
+    fill_recip(r, a.n_k, a.K, a.Vbeta);
+    for (int i = lane; i < bw; i += 32) bits[i] = 0u;
+    __syncthreads();
+    // the first kOrderList topics by (beta * r_k desc, k asc): repeated CTA-wide arg-max
+    const int L = min(kOrderList, a.K);
+    float pv = __int_as_float(0x7f800000);  // the previous pick; the next is the best ranked after it
+    int pk = -1;
+    for (int n = 0; n < L; ++n) {
+        float bv = -1.0f;
+        int bk = 0x7fffffff;
+        for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+            const float v = fmul(a.beta, r[k]);
+            if (ranks_above(pv, pk, v, k) && ranks_above(v, k, bv, bk)) { bv = v; bk = k; }
+        }
+        warp_argmax(bv, bk);
+        if (lane == 0) { red_v[wid] = bv; red_k[wid] = bk; }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            float v = red_v[0];
+            int k = red_k[0];
+            for (int i = 1; i < warps; ++i)
+                if (ranks_above(red_v[i], red_k[i], v, k)) { v = red_v[i]; k = red_k[i]; }
+            order[n] = k;
+        }
+        __syncthreads();
+        pk = order[n];
+        pv = fmul(a.beta, r[pk]);
+    }
+    for (int w = a.Vd + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
+        const int s = w - a.Vd;
+        const uint32_t* ent = a.swt_ent + __ldg(a.swt_off + s);
+        const uint32_t nnz = __ldg(a.swt_nnz + s);
+        float a1 = -1.0f, a2 = -1.0f, a3 = -1.0f;
+        int i1 = 0x7fffffff, i2 = 0x7fffffff, i3 = 0x7fffffff;
+        for (uint32_t e = lane; e < nnz; e += 32) {
+            const uint32_t en = __ldg(ent + e);
+            const int k = (int)(en >> 16);
+            atomicOr(&bits[k >> 5], 1u << (k & 31));
+            top3_insert(fmul(fadd(u2f(en & 0xffffu), a.beta), r[k]), k, a1, i1, a2, i2, a3, i3);
+        }
+        __syncwarp();
+        // the best three topics outside the word: the first three of the CTA's order that
+        // the word lacks (lane j looks at entry j), or, if the list runs out, every topic
+        int found = 0, o0 = 0, o1 = 0, o2 = 0;
+        for (int b = 0; b < L && found < 3; b += 32) {
+            const int j = b + lane;
+            const int kj = j < L ? order[j] : 0;
+            const bool out = j < L && !((bits[kj >> 5] >> (kj & 31)) & 1u);
+            for (unsigned m = __ballot_sync(FULL, out); m && found < 3; m &= m - 1u) {
+                const int k = __shfl_sync(FULL, kj, __ffs(m) - 1);
+                if (found == 0) o0 = k;
+                else if (found == 1) o1 = k;
+                else o2 = k;
+                ++found;
+            }
+        }
+        if (found == 3) {
+            if (lane == 0) {
+                top3_insert(fmul(a.beta, r[o0]), o0, a1, i1, a2, i2, a3, i3);
+                top3_insert(fmul(a.beta, r[o1]), o1, a1, i1, a2, i2, a3, i3);
+                top3_insert(fmul(a.beta, r[o2]), o2, a1, i1, a2, i2, a3, i3);
+            }
+        } else {
+            for (int k = lane; k < a.K; k += 32)
+                if (!((bits[k >> 5] >> (k & 31)) & 1u)) top3_insert(fmul(a.beta, r[k]), k, a1, i1, a2, i2, a3, i3);
+        }
+        float v[3];
+        int kk[3];
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            float bv = a1;
+            int bk = i1;
+            warp_argmax(bv, bk);
+            v[q] = bv;
+            kk[q] = bk;
+            if (i1 == bk) {
+                a1 = a2; i1 = i2;
+                a2 = a3; i2 = i3;
+                a3 = -1.0f; i3 = 0x7fffffff;
+            }
+        }
+        const int k1 = kk[0];
+        // prefix popcounts for the rank of a topic among the word's entries
+        uint32_t carry = 0;
+        for (int wb = 0; wb < bw; wb += 32) {
+            const int i = wb + lane;
+            const uint32_t c = i < bw ? (uint32_t)__popc(bits[i]) : 0u;
+            uint32_t incl = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t t = __shfl_up_sync(FULL, incl, off);
+                if (lane >= off) incl += t;
+            }
+            if (i < bw) pre[i] = (uint16_t)(carry + incl - c);
+            carry += __shfl_sync(FULL, incl, 31);
+        }
+        __syncwarp();
+        float ql = 0.0f;
+        for (int k = lane; k < a.K; k += 32) {
+            if (k == k1) continue;
+            const uint32_t bword = bits[k >> 5], m = 1u << (k & 31);
+            float phi;
+            if (bword & m) {
+                const uint32_t en = __ldg(ent + pre[k >> 5] + __popc(bword & (m - 1u)));
+                phi = fmul(fadd(u2f(en & 0xffffu), a.beta), r[k]);
+            } else {
+                phi = fmul(a.beta, r[k]);
+            }
+            ql = ffma(a.alpha, phi, ql);
+        }
+        const float qp = warp_ks_scan(ql, lane);
+        const float Q = __shfl_sync(FULL, qp, 31);
+        a.st_ql[(size_t)w * 32 + lane] = ql;
+        if (lane == 0) {
+            a.st_top2[w] = ((uint32_t)kk[1] << 16) | (uint32_t)k1;
+            a.st_k3[w] = (uint32_t)kk[2];
+            a.st_phi[w] = make_float4(v[0], v[1], v[2], Q);
+        }
+        __syncwarp();
+        for (uint32_t e = lane; e < nnz; e += 32) bits[(__ldg(ent + e) >> 16) >> 5] = 0u;
+        __syncwarp();
+    }
+}
+
 // Fixed-order FP64 reduction of the per-tile LL partials (one CTA of 1024 threads).
 // Replaces LDATrainPerplexityReduce (EZLDA/utility.cu:2106-2151).
 __global__ void __launch_bounds__(1024) k_ll_reduce(const double* __restrict__ in, int n, double* out) {

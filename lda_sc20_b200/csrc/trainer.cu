@@ -76,7 +76,9 @@ struct lda_trainer {
 
     int64_t dt_cap = 0, swt_cap = 0;
     size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0, smem_dense = 0, smem_sparse = 0;
+    size_t smem_stats_sparse = 0;
     int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_dense = 0, grid_sparse = 0;
+    int grid_stats_sparse = 0;
 
     std::vector<void*> allocs;
     int64_t bytes = 0, budget = 0;
@@ -502,6 +504,11 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return rc;
         T.grid_dense = std::min(g0, g1);
         T.grid_sparse = std::min(g2, g3);
+        T.smem_stats_sparse = dev::stats_sparse_smem(T.K, kLargeWarps);
+        CUDA_TRY(raise_smem_limit((const void*)dev::k_word_stats_sparse_large, T.smem_stats_sparse));
+        if ((rc = occupancy_grid((const void*)dev::k_word_stats_sparse_large, lt, T.smem_stats_sparse, T.num_sms,
+                                 &T.grid_stats_sparse)))
+            return rc;
     }
     T.grid_stats = (int)std::max<int64_t>(1, std::min<int64_t>(T.grid_stats, (V + T.warps - 1) / T.warps));
     CUDA_TRY(cudaDeviceSynchronize());
@@ -601,8 +608,25 @@ extern "C" int lda_max_topic(lda_trainer* t) {
     CUDA_TRY(cudaSetDevice(t->device));
     t->begin_stage(1);
     const dev::StatsArgs a = stats_args(t);
-    dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
-    CUDA_TRY(cudaGetLastError());
+    if (!t->large) {
+        dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    } else {
+        // dense words from their columns, sparse words without one
+        if (t->Vd > 0) {
+            dev::StatsArgs ad = a;
+            ad.V = t->Vd;
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats, (t->Vd + t->warps - 1) / t->warps));
+            dev::k_word_stats<<<grid, 32 * t->warps, t->smem_stats, t->stream>>>(ad);
+            CUDA_TRY(cudaGetLastError());
+        }
+        if (t->V > t->Vd) {
+            const int64_t ns = t->V - t->Vd;
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats_sparse, (ns + kLargeWarps - 1) / kLargeWarps));
+            dev::k_word_stats_sparse_large<<<grid, 32 * kLargeWarps, t->smem_stats_sparse, t->stream>>>(a);
+            CUDA_TRY(cudaGetLastError());
+        }
+    }
     t->end_stage();
     return LDA_OK;
 }

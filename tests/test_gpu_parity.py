@@ -322,3 +322,47 @@ def test_host_iterate_pinned_buffers(stream_mode, chunk_range):
     if chunk_range:
         t0, t1 = (int(x) for x in c.chunk_tok()[list(chunk_range)])
         assert np.array_equal(zout[:t0], z[:t0]) and np.array_equal(zout[t1:], z[t1:])
+
+
+@pytest.mark.parametrize("dense_kind,dense_param", [(0, 0.0), (1, 0.05)])
+def test_large_k_word_stats_bit_exact(dense_kind, dense_param):
+    """Above 2048 topics sparse words get their statistics without a column (own topics
+    plus the CTA's order of beta * r_k); they must equal the oracle's column-based ones."""
+    K = 4096
+    c = L.Corpus.generate(L.corpus_config("c0", num_docs=400, vocab=900, K=K, num_chunks=2,
+                                          dense_kind=dense_kind, dense_param=dense_param))
+    tr, o = _setup(c, K)
+    tr.iterate(2)
+    z = tr.topics()
+    o.rebuild(z)
+    tr.update_wt()
+    tr.max_topic()
+    tr.sync()
+    for a, b, n in zip(tr.word_stats(), o.word_stats(), ("top2", "k3", "phi4", "ql")):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
+
+
+def test_large_k_word_stats_fallback_scan():
+    """A sparse word holding every topic at the head of the beta * r_k order (the topics
+    with the fewest tokens) makes the statistics fall back to scanning all topics."""
+    K = 4096
+    # word "a": one token on each of topics 0..99; word "b": two tokens on every other topic
+    wa = [0] * 100
+    ta = list(range(100))
+    wb = [1] * (2 * (K - 100))
+    tb = [k for k in range(100, K) for _ in range(2)]
+    words = np.array(wa + wb, dtype=np.int32)
+    topics = np.array(ta + tb, dtype=np.uint16)
+    doc_off = np.arange(0, len(words) + 1, 400, dtype=np.int64)
+    doc_off[-1] = len(words)
+    if doc_off[-2] == doc_off[-1]:
+        doc_off = doc_off[:-1]
+    c = L.Corpus.from_docs(doc_off, words, vocab=2, K=K, topics=topics, num_chunks=1)
+    tr, o = _setup(c, K)
+    o.rebuild(c.topics())
+    tr.update_wt()
+    tr.max_topic()
+    tr.sync()
+    assert c.info.num_dense == 1
+    for a, b, n in zip(tr.word_stats(), o.word_stats(), ("top2", "k3", "phi4", "ql")):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), n
