@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
 
 // Sampler: warp per tile, tiles taken from an atomic counter.
 template <bool LL, int QB = 1>
-__global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_t(SampleArgs a) {
+__global__ void __launch_bounds__(32 * kSampleWarps, LL ? LDA_SAMPLE_LL_MIN_BLOCKS
+                                                       : (QB == 1 ? LDA_SAMPLE_MIN_BLOCKS : LDA_SAMPLE_QB_MIN_BLOCKS))
+k_sample_t(SampleArgs a) {
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* r = smf;
@@ -138,7 +140,7 @@ __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
 #endif
 
 template <bool LL, int QB>
-__global__ void __launch_bounds__(256, LDA_SAMPLE_MIN_BLOCKS) k_sample_sparse_large(SampleArgs a) {
+__global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_sparse_large(SampleArgs a) {
     extern __shared__ float smf[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bw = large_bit_words(a.K), pw = large_pre_words(a.K);

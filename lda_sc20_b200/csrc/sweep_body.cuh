@@ -346,8 +346,25 @@ constexpr int kLargeK = 2048;
 // cost no registers in the sampling loop.
 enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE, C_ROWS, C_RENT, C_NUM };
 
+// Warps per CTA of the K <= 2048 sampler (one shared word column per warp), and the CTAs
+// per SM it is compiled for: the register cap is 65536 / (32 * warps * blocks) per
+// thread.  The LL-mode kernel (its FP64 term) and the K > 1024 kernel (four Q rounds per
+// batch) keep more state live and are compiled for fewer.
+#ifndef LDA_SAMPLE_WARPS
+#define LDA_SAMPLE_WARPS 8
+#endif
+constexpr int kSampleWarps = LDA_SAMPLE_WARPS;
 #ifndef LDA_SAMPLE_MIN_BLOCKS
-#define LDA_SAMPLE_MIN_BLOCKS 4
+#define LDA_SAMPLE_MIN_BLOCKS 5
+#endif
+#ifndef LDA_SAMPLE_QB_MIN_BLOCKS
+#define LDA_SAMPLE_QB_MIN_BLOCKS 4
+#endif
+#ifndef LDA_SAMPLE_LL_MIN_BLOCKS
+#define LDA_SAMPLE_LL_MIN_BLOCKS 4
+#endif
+#ifndef LDA_SPARSE_LARGE_MIN_BLOCKS
+#define LDA_SPARSE_LARGE_MIN_BLOCKS 4
 #endif
 
 // Branch taken by a token (counters only).

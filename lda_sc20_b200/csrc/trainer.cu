@@ -27,7 +27,14 @@ namespace {
 #ifndef LDA_SAMPLE_TILE
 #define LDA_SAMPLE_TILE 512
 #endif
-constexpr int kSampleTile = LDA_SAMPLE_TILE;  // tokens per sampler tile (a word's column is rebuilt per tile)
+constexpr int kSampleTile = LDA_SAMPLE_TILE;  // most tokens per sampler tile (a word's column is rebuilt per tile)
+constexpr int kSampleTileMin = 64;            // fewest tokens per tile that a chunk's tile size goes down to
+#ifndef LDA_TILES_PER_WARP
+#define LDA_TILES_PER_WARP 2
+#endif
+// A chunk's sampler tiles are sized so that each resident warp gets about this many:
+// with fewer, the launch ends with the longest tile while most warps sit idle.
+constexpr int kTilesPerWarp = LDA_TILES_PER_WARP;
 constexpr int kDenseTileLarge = 2048;         // dense-word tiles above kLargeK topics (one CTA per tile)
 constexpr int kLargeWarps = 8;                // warps per CTA of the large-K sampler kernels
 constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
@@ -44,6 +51,7 @@ struct lda_trainer {
     int device = 0;
     cudaStream_t own_stream = nullptr, stream = nullptr;
     int K = 0, Vd = 0, C = 0, warps = 8, num_sms = 0;
+    int swarps = 8;  // warps per CTA of the K <= 2048 sampler
     float alpha = 0, beta = 0, Vbeta = 0;
     uint64_t seed = 0;
     uint32_t iter = 0;
@@ -77,7 +85,7 @@ struct lda_trainer {
     int64_t dt_cap = 0, swt_cap = 0;
     size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0, smem_dense = 0, smem_sparse = 0;
     size_t smem_stats_sparse = 0;
-    int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_dense = 0, grid_sparse = 0;
+    int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_sample_ll = 0, grid_dense = 0, grid_sparse = 0;
     int grid_stats_sparse = 0;
 
     std::vector<void*> allocs;
@@ -297,9 +305,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     auto sample_bytes = [&](int w) { return (size_t)T.K * 4 + (size_t)w * (dev::col_words(T.K) * 4 + 16 * sizeof(uint32_t)); };
     T.large = T.K > dev::kLargeK;
     if (!T.large) {
-        while (T.warps > 1 && sample_bytes(T.warps) > (size_t)max_smem) --T.warps;
-        if (sample_bytes(T.warps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
-        T.smem_sample = sample_bytes(T.warps);
+        T.swarps = dev::kSampleWarps;
+        while (T.swarps > 1 && sample_bytes(T.swarps) > (size_t)max_smem) --T.swarps;
+        if (sample_bytes(T.swarps) > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", T.K);
+        T.smem_sample = sample_bytes(T.swarps);
     } else {
         T.smem_dense = dev::dense_large_smem(T.K, kLargeWarps);
         T.smem_sparse = dev::sparse_large_smem(T.K, kLargeWarps);
@@ -335,17 +344,32 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     }
     T.swt_cap = run;
     // sampler tiles per chunk, largest first (for K > kLargeK: dense-word tiles, then
-    // sparse-word tiles, each largest first)
+    // sparse-word tiles, each largest first).  For K <= kLargeK a chunk's tile size is
+    // its tokens / (kTilesPerWarp x the sampler's resident warps), rounded up to 32 and
+    // kept within [kSampleTileMin, kSampleTile].
+    int64_t resident_warps = 0;
+    if (!T.large) {
+        CUDA_TRY(raise_smem_limit(sample_kernel(false, T.K), T.smem_sample));
+        int g = 0, orc = occupancy_grid(sample_kernel(false, T.K), 32 * T.swarps, T.smem_sample, T.num_sms, &g);
+        if (orc) return orc;
+        resident_warps = (int64_t)g * T.swarps;
+    }
     std::vector<int4> st;
     T.s_tile_base.assign(T.C + 1, 0);
     T.s_tile_split.assign(T.C, 0);
     auto by_size = [](const int4& a, const int4& b) { return a.z > b.z; };
     for (int ch = 0; ch < T.C; ++ch) {
         std::vector<int4> ct, cs;
+        int64_t tile_ch = kSampleTile;
+        if (!T.large) {
+            const int64_t per = kTilesPerWarp * std::max<int64_t>(resident_warps, 1);
+            const int64_t want = ((T.chunk_tok[ch + 1] - T.chunk_tok[ch] + per - 1) / per + 31) / 32 * 32;
+            tile_ch = std::min<int64_t>(kSampleTile, std::max<int64_t>(kSampleTileMin, want));
+        }
         for (int64_t w = 0; w < V; ++w) {
             const int64_t n = c->seg_cnt[(size_t)ch * V + w], o = c->seg_off[(size_t)ch * V + w];
             const bool dense = w < T.Vd;
-            const int64_t tile = T.large && dense ? kDenseTileLarge : kSampleTile;
+            const int64_t tile = T.large && dense ? kDenseTileLarge : tile_ch;
             for (int64_t p = 0; p < n; p += tile) {
                 const int4 v = make_int4((int)w, (int)(o + p), (int)std::min<int64_t>(tile, n - p), dense);
                 (T.large && !dense ? cs : ct).push_back(v);
@@ -485,11 +509,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
     if (!T.large) {
-        int grid_ll = 0;
         for (bool ll : {false, true}) CUDA_TRY(raise_smem_limit(sample_kernel(ll, T.K), T.smem_sample));
-        if ((rc = occupancy_grid(sample_kernel(false, T.K), threads, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
-        if ((rc = occupancy_grid(sample_kernel(true, T.K), threads, T.smem_sample, T.num_sms, &grid_ll))) return rc;
-        T.grid_sample = std::min(T.grid_sample, grid_ll);
+        const int st = 32 * T.swarps;
+        if ((rc = occupancy_grid(sample_kernel(false, T.K), st, T.smem_sample, T.num_sms, &T.grid_sample))) return rc;
+        if ((rc = occupancy_grid(sample_kernel(true, T.K), st, T.smem_sample, T.num_sms, &T.grid_sample_ll))) return rc;
     } else {
         const int lt = 32 * kLargeWarps;
         int g0 = 0, g1 = 0, g2 = 0, g3 = 0;
@@ -741,8 +764,9 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
     }
     CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(unsigned), q));
     if (n > 0) {
-        const int grid = std::max(1, std::min(t->grid_sample, (n + t->warps - 1) / t->warps));
-        launch_sample(a.ll_mode != 0, t->K, grid, 32 * t->warps, t->smem_sample, q, a);
+        const int cap = a.ll_mode ? t->grid_sample_ll : t->grid_sample;
+        const int grid = std::max(1, std::min(cap, (n + t->swarps - 1) / t->swarps));
+        launch_sample(a.ll_mode != 0, t->K, grid, 32 * t->swarps, t->smem_sample, q, a);
         CUDA_TRY(cudaGetLastError());
     }
     t->chunk_sampled_ll[chunk] = ll_mode != 0;
@@ -1303,7 +1327,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     CUDA_TRY(cudaDeviceGetAttribute(&max_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, device));
     CUDA_TRY(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device));
     const int64_t row = (int64_t)io->K * 4;
-    const int warps = (int)std::min<int64_t>(8, ((int64_t)max_smem - 2048) / (row + 256) - 1);
+    const int warps = (int)std::min<int64_t>(std::min(8, dev::kSampleWarps), ((int64_t)max_smem - 2048) / (row + 256) - 1);
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
     const size_t smem = (size_t)io->K * 4 + (size_t)warps * (dev::col_words(io->K) * 4 + 16 * sizeof(uint32_t));
     if (warps < 1 || smem > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
