@@ -203,6 +203,41 @@ __device__ __forceinline__ int warp_level2_rounds(uint32_t n, float t2, int fall
     return last >= 0 ? last : fallback;
 }
 
+// Rounds of the Q-bucket search of one lane slot ls whose (round total, largest lane
+// prefix) pairs the dense-word sampler keeps per tile: R = ceil(ceil(K/32) / 32) rounds of
+// 32 slots, for 2 <= R <= 16 (above that the table is not kept).
+__host__ __device__ __forceinline__ int qtab_rounds(int K) {
+    const int R = ((K + 31) / 32 + 31) / 32;
+    return (R >= 2 && R <= 16) ? R : 0;
+}
+
+// warp_level2_rounds (QB = 1 order) with the rounds' totals and largest lane prefixes known
+// (tab[r] = (KS total of round r, max over lanes of its KS prefix)).  Round r can hold the
+// crossing only if t2 < carry + max prefix; other rounds only add their total to the carry,
+// with the same additions in the same order, so the round that is evaluated sees the same
+// carry and gives the same topic.  Returns -1 when no evaluated round crosses; the caller
+// then runs the full search, which also finds the fallback topic.
+template <class Slot>
+__device__ __forceinline__ int warp_level2_table(uint32_t n, float t2, int lane, Slot slot, const float2* tab) {
+    const uint32_t R = (n + 31u) >> 5;
+    float carry = 0.0f;
+    for (uint32_t r = 0; r < R; ++r) {
+        const float2 tm = tab[r];
+        if (t2 < fadd(carry, tm.y)) {
+            int key = -1;
+            float ks = 0.0f;
+            bool ok = false;
+            const uint32_t i = 32u * r + lane;
+            if (i < n) slot(i, key, ks, ok);
+            ks = warp_ks_scan(ks, lane);
+            const unsigned f = __ballot_sync(FULL, ok && t2 < fadd(carry, ks));
+            if (f) return __shfl_sync(FULL, key, __ffs(f) - 1);
+        }
+        carry = fadd(carry, tm.x);
+    }
+    return -1;
+}
+
 // The sampler's view of the tile's word column: colz(k) = phi_k of the word with its max
 // topic zeroed.  ColShared reads a column built in shared memory (skewed layout, with the
 // max topic's slot already zeroed).

@@ -131,8 +131,14 @@ __host__ __device__ __forceinline__ size_t sparse_large_smem(int K, int warps) {
 
 // Shared memory of the dense-word kernel: the shared column, the warps' counter rows and
 // their LL partials (the reciprocals are formed while the column is built).
+#ifndef LDA_QTAB
+#define LDA_QTAB 1
+#endif
+// Shared memory of the dense-word sampler: the word column, the warps' counter rows, their
+// LL partials and (when qtab_rounds(K) > 0) the Q-round table of 32 x R float2.
 __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
-    return (((size_t)col_words(K) * 4 + (size_t)warps * C_NUM * 4 + 7) & ~(size_t)7) + (size_t)warps * 8;
+    return (((size_t)col_words(K) * 4 + (size_t)warps * C_NUM * 4 + 7) & ~(size_t)7) + (size_t)warps * 8 +
+           (LDA_QTAB ? (size_t)32 * qtab_rounds(K) * sizeof(float2) : 0);
 }
 
 #ifndef LDA_DENSE_LARGE_MIN_BLOCKS
@@ -220,6 +226,8 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
     uint32_t* ctr = ctr_all + C_NUM * wid;
     double* wll = reinterpret_cast<double*>(
         (reinterpret_cast<uintptr_t>(ctr_all + C_NUM * warps) + 7) & ~(uintptr_t)7);
+    const int qr = LDA_QTAB ? qtab_rounds(a.K) : 0;
+    float2* qtab = reinterpret_cast<float2*>(wll + warps);
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();
     for (;;) {
@@ -243,12 +251,30 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
             ctr[C_TDENSE] += 1u;
         }
         __syncthreads();
+        if (qr) {
+            // the Q-round table of this word: for lane slot ls and round r, the KS total and the
+            // largest KS prefix of alpha * colz(ls + 32 * (32 r + l)), l = 0..31 (slots past the
+            // lane's last topic add 0), the terms and scan of warp_level2_rounds
+            const ColShared cv{col};
+            for (int job = wid; job < 32 * qr; job += warps) {
+                const int ls = job / qr, r = job - ls * qr;
+                const uint32_t n = (uint32_t)((a.K - ls + 31) / 32), i = 32u * (uint32_t)r + (uint32_t)lane;
+                const float term = i < n ? fmul(a.alpha, cv(ls + 32 * (int)i)) : 0.0f;
+                const float ks = warp_ks_scan(term, lane);
+                float mx = ks;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, off));
+                const float tot = __shfl_sync(FULL, ks, 31);
+                if (lane == 0) qtab[job] = make_float2(tot, mx);
+            }
+            __syncthreads();
+        }
         const float4 ph = __ldg(a.st_phi + w);
         const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
         const float QP = warp_ks_scan(QL, lane);
         const float Q = __shfl_sync(FULL, QP, 31);
         double ll = sample_groups<LL, QB>(a, (uint32_t)t.y, (uint32_t)t.z, 32u * wid, 32u * warps, a.iter, maxK, ph, QL,
-                                          QP, Q, ColShared{col}, ctr, lane);
+                                          QP, Q, ColShared{col}, ctr, lane, qr ? qtab : nullptr, qr);
         if (LL) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);

@@ -376,7 +376,8 @@ enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 template <bool LL, int QB, class View>
 __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t start, uint32_t cnt, uint32_t g0,
                                                 uint32_t gstep, uint32_t iter, int maxK, const float4 ph, float QL,
-                                                float QP, float Q, const View& colz, uint32_t* ctr, int lane) {
+                                                float QP, float Q, const View& colz, uint32_t* ctr, int lane,
+                                                const float2* qtab = nullptr, int qrounds = 0) {
     double ll = 0.0;
     uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
     const uint32_t* row = a.dt_ent;
@@ -458,13 +459,15 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 const int K = a.K;
                 const float alpha = a.alpha;
                 const uint32_t n = (uint32_t)((K - ls + 31) / 32);
-                const int zq = warp_level2_rounds<QB>(n, t2, maxK, lane, [&](uint32_t i, int& key, float& term, bool& ok) {
+                auto slot = [&](uint32_t i, int& key, float& term, bool& ok) {
                     const int k = ls + 32 * (int)i;
                     const float cz = colz(k);
                     key = k;
                     term = fmul(alpha, cz);
                     ok = cz > 0.0f;
-                });
+                };
+                int zq = qtab ? warp_level2_table(n, t2, lane, slot, qtab + ls * qrounds) : -1;
+                if (zq < 0) zq = warp_level2_rounds<QB>(n, t2, maxK, lane, slot);
                 if (lane == j) {
                     kind = BR_Q;
                     znew = zq;
