@@ -106,27 +106,30 @@ struct ColBits {
     const uint32_t* bits;  // ceil(K/32) words
     const uint16_t* pre;   // set bits before each word
     const uint32_t* ent;   // the word's row, (k << 16) | count
-    const float* r;
+    const float* r;        // reciprocals in the skewed layout: r_k at col_skew(k)
     float beta;
     int maxK;
     __device__ __forceinline__ float operator()(int k) const {
         if (k == maxK) return 0.0f;
         const uint32_t b = bits[k >> 5], m = 1u << (k & 31);
+        const float rk = r[col_skew(k)];
         if (b & m) {
             const uint32_t e = __ldg(ent + pre[k >> 5] + __popc(b & (m - 1u)));
-            return fmul(fadd(u2f(e & 0xffffu), beta), r[k]);
+            return fmul(fadd(u2f(e & 0xffffu), beta), rk);
         }
-        return fmul(beta, r[k]);
+        return fmul(beta, rk);
     }
 };
 
 __host__ __device__ __forceinline__ int large_bit_words(int K) { return (K + 31) >> 5; }
 __host__ __device__ __forceinline__ int large_pre_words(int K) { return ((K + 31) >> 5) + 1 & ~1; }
 
-// Shared memory of the sparse-word kernel: r[K], then per warp the bitmap, then per warp
-// the prefix counts (uint16, an even number per warp), then per warp the counter row.
+// Shared memory of the sparse-word kernel: the reciprocals in the skewed column layout
+// (col_words(K) floats: a Q round's 32 topics k, k + 32, ... then sit in 32 banks), then
+// per warp the bitmap, then per warp the prefix counts (uint16, an even number per warp),
+// then per warp the counter row.
 __host__ __device__ __forceinline__ size_t sparse_large_smem(int K, int warps) {
-    return (size_t)K * 4 + (size_t)warps * (large_bit_words(K) * 4 + large_pre_words(K) * 2 + C_NUM * 4);
+    return (size_t)col_words(K) * 4 + (size_t)warps * (large_bit_words(K) * 4 + large_pre_words(K) * 2 + C_NUM * 4);
 }
 
 // Shared memory of the dense-word kernel: the shared column, the warps' counter rows and
@@ -151,14 +154,16 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int bw = large_bit_words(a.K), pw = large_pre_words(a.K);
     float* r = smf;
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smf + a.K) + (size_t)bw * wid;
-    uint16_t* pre = reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(smf + a.K) + (size_t)bw * warps) +
+    float* rend = smf + col_words(a.K);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(rend) + (size_t)bw * wid;
+    uint16_t* pre = reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(rend) + (size_t)bw * warps) +
                     (size_t)pw * wid;
-    uint32_t* ctr = reinterpret_cast<uint32_t*>(reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(smf + a.K) +
+    uint32_t* ctr = reinterpret_cast<uint32_t*>(reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(rend) +
                                                                             (size_t)bw * warps) +
                                                 (size_t)pw * warps) +
                     C_NUM * wid;
-    fill_recip(r, a.n_k, a.K, a.Vbeta);
+    for (int k = threadIdx.x; k < a.K; k += blockDim.x)
+        r[col_skew(k)] = __fdiv_rn(1.0f, fadd(__int2float_rn(a.n_k[k]), a.Vbeta));
     for (int i = lane; i < bw; i += 32) bits[i] = 0u;
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();
