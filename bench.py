@@ -91,9 +91,12 @@ def measured_peaks():
         return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the sampler from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "k_sample_c1_traffic.json")
+def ncu_traffic(preset: str, chunks: int = 0):
+    """Per-launch DRAM bytes of the sampler from the committed ncu summary of this workload
+    (profiles/k_sample_<preset>_traffic.json), if there is one for its default chunking."""
+    if chunks:
+        return None
+    path = os.path.join(ROOT, "profiles", f"k_sample_{preset}_traffic.json")
     try:
         with open(path) as f:
             return json.load(f)
@@ -400,7 +403,7 @@ def run_ours(args, world, rank, local):
         achieved = None  # the timed stage spans the chunk copies, doc-row rebuilds and sampling
     peaks, peak_src = measured_peaks()
     peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
-    traffic = ncu_traffic()
+    traffic = ncu_traffic(args.preset, args.chunks)
 
     # end to end through the C ABI with pinned host buffers: upload topics, sweep, download
     e2e = None
