@@ -160,8 +160,7 @@ __global__ void __launch_bounds__(256) kb_sample(BatchArgs b) {
 __global__ void __launch_bounds__(1024) kb_ll(const SampleArgs* sm, double* out) {
     __shared__ double s[1024];
     const SampleArgs& a = sm[blockIdx.x];
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < a.ntiles; i += blockDim.x) acc += a.tile_ll[i];
+    const double acc = strided_sum(a.tile_ll, a.ntiles);
     s[threadIdx.x] = acc;
     __syncthreads();
     for (int h = blockDim.x >> 1; h > 0; h >>= 1) {

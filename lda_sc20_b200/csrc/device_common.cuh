@@ -29,6 +29,23 @@ __device__ __forceinline__ float warp_ks_scan(float v, int lane) {
     return v;
 }
 
+// Thread t's sum of in[t], in[t + blockDim.x], ... in that order (the first stage of the
+// fixed-order FP64 LL reductions).  Eight loads are issued before their eight additions.
+__device__ __forceinline__ double strided_sum(const double* __restrict__ in, int n) {
+    const int st = blockDim.x;
+    double acc = 0.0;
+    int i = threadIdx.x;
+    for (; i + 7 * st < n; i += 8 * st) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = __ldg(in + i + u * st);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) acc += v[u];
+    }
+    for (; i < n; i += st) acc += __ldg(in + i);
+    return acc;
+}
+
 // Philox4x32-10 (Salmon et al., SC'11), first output word.
 __device__ __forceinline__ uint32_t philox_x0(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
                                               uint32_t k0, uint32_t k1) {

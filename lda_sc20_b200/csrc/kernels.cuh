@@ -463,8 +463,7 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
 // Replaces LDATrainPerplexityReduce (EZLDA/utility.cu:2106-2151).
 __global__ void __launch_bounds__(1024) k_ll_reduce(const double* __restrict__ in, int n, double* out) {
     __shared__ double s[1024];
-    double acc = 0.0;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) acc += in[i];
+    const double acc = strided_sum(in, n);
     s[threadIdx.x] = acc;
     __syncthreads();
     for (int h = blockDim.x >> 1; h > 0; h >>= 1) {
