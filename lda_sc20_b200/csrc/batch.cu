@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(256) kb_wt(BatchArgs b) {
         if (i >= b.n_wt) break;
         const uint2 w = b.wt_work[i];
         const WtArgs& a = b.wt[w.x];
-        wt_tile(a, a.tiles[w.y], hist, bits, reinterpret_cast<unsigned*>(a.n_k), lane);
+        wt_tile(a, a.tiles[w.y], Hist<false>{hist}, bits, reinterpret_cast<unsigned*>(a.n_k), lane);
     }
 }
 
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(256) kb_dt(BatchArgs b) {
         if (i >= b.n_dt) break;
         const uint4 u = b.dt_work[i];
         const DtArgs& a = b.dt[u.x];
-        for (uint32_t d = u.y; d < u.y + u.z; ++d) dt_doc(a, d, hist, bits, lane);
+        for (uint32_t d = u.y; d < u.y + u.z; ++d) dt_doc(a, d, Hist<false>{hist}, bits, lane);
     }
 }
 

@@ -72,11 +72,40 @@ __device__ __forceinline__ float token_uniform(uint32_t seed_lo, uint32_t seed_h
     return u2f(x >> 8) * 0x1p-24f;
 }
 
+// A warp-private shared histogram over topics [0, K).  Hist<false>: one 32-bit count per
+// topic.  Hist<true>: 16-bit counts, two per 32-bit word (half the shared memory, so twice
+// the warps at large K), for counts known to stay below 2^16.  Adds are 32-bit atomics on
+// the containing word with the count shifted into its half; they never carry into the
+// other half.  Reads and clears use the 16-bit view; the two topics of a word (k, k ^ 1)
+// share a bitmap word, so one lane owns both when a histogram is read out and cleared.
+template <bool P16>
+struct Hist;
+template <>
+struct Hist<false> {
+    uint32_t* h;
+    __host__ __device__ static constexpr int words(int K) { return K; }
+    __device__ __forceinline__ uint32_t add(uint32_t k, uint32_t c) const { return atomicAdd(h + k, c); }
+    __device__ __forceinline__ uint32_t get(uint32_t k) const { return h[k]; }
+    __device__ __forceinline__ void clear(uint32_t k) const { h[k] = 0u; }
+};
+template <>
+struct Hist<true> {
+    uint32_t* h;
+    __host__ __device__ static constexpr int words(int K) { return (K + 1) >> 1; }
+    __device__ __forceinline__ uint32_t add(uint32_t k, uint32_t c) const {
+        const uint32_t sh = (k & 1u) << 4;
+        return (atomicAdd(h + (k >> 1), c << sh) >> sh) & 0xffffu;
+    }
+    __device__ __forceinline__ uint32_t get(uint32_t k) const { return reinterpret_cast<const uint16_t*>(h)[k]; }
+    __device__ __forceinline__ void clear(uint32_t k) const { reinterpret_cast<uint16_t*>(h)[k] = 0; }
+};
+
 // Histogram of topics z[start, start + cnt) into the warp's shared `hist`; a topic whose
 // count leaves zero also gets its bit in `bits` (ceil(K/32) words).  Four 32-token steps
 // of topic loads are in flight together.
+template <class H>
 __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uint32_t start, uint32_t cnt,
-                                             uint32_t* hist, uint32_t* bits, int K, int lane, int* err) {
+                                             const H& hist, uint32_t* bits, int K, int lane, int* err) {
     for (uint32_t base = 0; base < cnt; base += 128) {
         uint32_t k[4];
 #pragma unroll
@@ -96,7 +125,7 @@ __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uin
             }
             const unsigned m = __match_any_sync(FULL, kk);
             if (valid && lane == __ffs(m) - 1) {
-                if (atomicAdd(&hist[kk], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
+                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
             }
         }
     }

@@ -14,14 +14,18 @@
 namespace lda {
 namespace dev {
 
-// Word-topic rebuild: warp per word tile, topic totals privatised per CTA.
+// Word-topic rebuild: warp per word tile, topic totals privatised per CTA.  P16: 16-bit
+// histogram counts (a dense tile holds at most 16,384 tokens and a sparse word fewer than
+// 65,536, so every count fits).
+template <bool P16>
 __global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
     extern __shared__ uint32_t smu[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = a.K + wt_bit_words(a.K);
+    const int hw = Hist<P16>::words(a.K);
+    const int per = hw + wt_bit_words(a.K);
     uint32_t* nk = smu;
-    uint32_t* hist = smu + a.K + (size_t)per * wid;
-    uint32_t* bits = hist + a.K;
+    const Hist<P16> hist{smu + a.K + (size_t)per * wid};
+    uint32_t* bits = hist.h + hw;
     for (int i = threadIdx.x; i < a.K + per * warps; i += blockDim.x) smu[i] = 0u;
     __syncthreads();
     for (;;) {
@@ -52,13 +56,16 @@ __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
     }
 }
 
-// Doc-topic rebuild: warp per doc of one chunk.
+// Doc-topic rebuild: warp per doc of one chunk.  P16: 16-bit histogram counts (a doc has
+// at most 65,535 tokens).
+template <bool P16>
 __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
     extern __shared__ uint32_t smu[];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int per = a.K + dt_bit_words(a.K);
-    uint32_t* hist = smu + (size_t)per * wid;
-    uint32_t* bits = hist + a.K;
+    const int hw = Hist<P16>::words(a.K);
+    const int per = hw + dt_bit_words(a.K);
+    const Hist<P16> hist{smu + (size_t)per * wid};
+    uint32_t* bits = hist.h + hw;
     for (int i = threadIdx.x; i < per * warps; i += blockDim.x) smu[i] = 0u;
     __syncthreads();
     for (uint32_t d = a.d_begin + blockIdx.x * warps + wid; d < a.d_end; d += gridDim.x * warps) {

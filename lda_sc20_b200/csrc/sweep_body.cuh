@@ -46,7 +46,8 @@ struct WtArgs {
 // shared array, or the model's global totals).
 __device__ __forceinline__ int wt_bit_words(int K) { return (K + 31) >> 5; }
 
-__device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t* hist, uint32_t* bits, unsigned* nk,
+template <class H>
+__device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, const H& hist, uint32_t* bits, unsigned* nk,
                                         int lane) {
     const int w = t.x;
     if (t.w & 1) {
@@ -78,10 +79,10 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t*
             while (m) {
                 const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
                 m &= m - 1u;
-                const uint32_t h = hist[k];
+                const uint32_t h = hist.get(k);
                 atomicAdd(row + k, (int)h);
                 atomicAdd(nk + k, h);
-                hist[k] = 0u;
+                hist.clear(k);
             }
         }
     } else {
@@ -104,10 +105,10 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, uint32_t*
             while (m) {
                 const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
                 m &= m - 1u;
-                const uint32_t h = hist[k];
+                const uint32_t h = hist.get(k);
                 out[p++] = (k << 16) | h;
                 atomicAdd(nk + k, h);
-                hist[k] = 0u;
+                hist.clear(k);
             }
         }
         if (lane == 0) a.swt_nnz[s] = nnz;
@@ -214,7 +215,8 @@ struct DtArgs {
 // exclusive scan of their popcounts places its entries, ascending k.
 __device__ __forceinline__ int dt_bit_words(int K) { return (K + 31) >> 5; }
 
-__device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hist, uint32_t* bits, int lane) {
+template <class H>
+__device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& hist, uint32_t* bits, int lane) {
     const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
     const uint32_t* dpos = a.dtok_pos + (b - a.tok_base);
     const uint32_t* dword = a.dtok_word + (b - a.tok_base);
@@ -240,7 +242,7 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hi
             }
             const unsigned m = __match_any_sync(FULL, kk);
             if (valid && lane == __ffs(m) - 1) {
-                if (atomicAdd(&hist[kk], (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
+                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
             }
         }
     }
@@ -259,7 +261,7 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hi
         for (int s = 0; s < 4; ++s) {
             if (pos[s] == 0xffffffffu) continue;
             const uint32_t k1 = t2[s] & 0xffffu, k2 = t2[s] >> 16;
-            const uint32_t c1 = k1 < (uint32_t)a.K ? hist[k1] : 0u, c2 = k2 < (uint32_t)a.K ? hist[k2] : 0u;
+            const uint32_t c1 = k1 < (uint32_t)a.K ? hist.get(k1) : 0u, c2 = k2 < (uint32_t)a.K ? hist.get(k2) : 0u;
             a.meta[pos[s] - a.tok_base] = (c2 << 16) | c1;
         }
     }
@@ -283,8 +285,8 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, uint32_t* hi
         while (m) {
             const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
             m &= m - 1u;
-            out[p++] = (k << 16) | hist[k];
-            hist[k] = 0u;
+            out[p++] = (k << 16) | hist.get(k);
+            hist.clear(k);
         }
     }
     if (lane == 0) a.dt_nnz[d] = nnz;

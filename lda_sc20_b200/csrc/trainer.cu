@@ -52,6 +52,7 @@ struct lda_trainer {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     int K = 0, Vd = 0, C = 0, warps = 8, num_sms = 0;
     int swarps = 8;  // warps per CTA of the K <= 2048 sampler
+    int warps_wt = 8, warps_dt = 8;  // warps per CTA of the word-topic and doc-topic rebuilds
     float alpha = 0, beta = 0, Vbeta = 0;
     uint64_t seed = 0;
     uint32_t iter = 0;
@@ -316,11 +317,22 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory (the dense-word sampler needs %zu bytes)", T.K,
                         T.smem_dense);
     }
-    auto wt_bytes = [&](int w) { return ((size_t)T.K + (size_t)w * (T.K + (T.K + 31) / 32)) * 4; };
-    while (T.warps > 1 && wt_bytes(T.warps) > (size_t)max_smem) --T.warps;
     T.smem_stats = (size_t)(T.warps + 1) * row;
-    T.smem_wt = wt_bytes(T.warps);
-    T.smem_dt = (size_t)T.warps * (T.K + (T.K + 31) / 32) * 4;
+    // the rebuilds' warp-private histograms hold 16-bit counts, two per word: a dense
+    // word-topic tile has kWtTile tokens, a sparse word fewer than 65,536 and a doc at most
+    // 65,535 (the corpus layout's limit), so every count fits.  Each rebuild takes as many
+    // warps per CTA (up to 8) as its shared memory allows.
+    const size_t bitw = (size_t)(T.K + 31) / 32;
+    auto wt_bytes = [&](int w) { return ((size_t)T.K + (size_t)w * (dev::Hist<true>::words(T.K) + bitw)) * 4; };
+    auto dt_bytes = [&](int w) { return (size_t)w * (dev::Hist<true>::words(T.K) + bitw) * 4; };
+    T.warps_wt = 8;
+    while (T.warps_wt > 1 && wt_bytes(T.warps_wt) > (size_t)max_smem) --T.warps_wt;
+    T.warps_dt = 8;
+    while (T.warps_dt > 1 && dt_bytes(T.warps_dt) > (size_t)max_smem) --T.warps_dt;
+    if (wt_bytes(T.warps_wt) > (size_t)max_smem || dt_bytes(T.warps_dt) > (size_t)max_smem)
+        return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory (count rebuilds)", T.K);
+    T.smem_wt = wt_bytes(T.warps_wt);
+    T.smem_dt = dt_bytes(T.warps_dt);
 
     // ---- host-side derived layout
     const int64_t N = T.N, V = T.V, D = T.D, Vs = V - T.Vd;
@@ -502,12 +514,14 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
 
     // ---- launch shapes: persistent grids sized by occupancy
     const int threads = 32 * T.warps;
-    for (auto kv : {std::make_pair((const void*)dev::k_wt_build, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
-                    std::make_pair((const void*)dev::k_dt_build, T.smem_dt)})
+    const void* wt_fn = (const void*)dev::k_wt_build<true>;
+    const void* dt_fn = (const void*)dev::k_dt_build<true>;
+    for (auto kv : {std::make_pair(wt_fn, T.smem_wt), std::make_pair((const void*)dev::k_word_stats, T.smem_stats),
+                    std::make_pair(dt_fn, T.smem_dt)})
         CUDA_TRY(raise_smem_limit(kv.first, kv.second));
-    if ((rc = occupancy_grid((const void*)dev::k_wt_build, threads, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
+    if ((rc = occupancy_grid(wt_fn, 32 * T.warps_wt, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
-    if ((rc = occupancy_grid((const void*)dev::k_dt_build, threads, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
+    if ((rc = occupancy_grid(dt_fn, 32 * T.warps_dt, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
     if (!T.large) {
         for (bool ll : {false, true}) CUDA_TRY(raise_smem_limit(sample_kernel(ll, T.K), T.smem_sample));
         const int st = 32 * T.swarps;
@@ -619,8 +633,8 @@ extern "C" int lda_update_wt(lda_trainer* t) {
     if (t->Vd > 0) CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
     CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
     const dev::WtArgs a = wt_args(t);
-    const int grid = std::max(1, std::min(t->grid_wt, (t->n_wtiles + t->warps - 1) / t->warps));
-    dev::k_wt_build<<<grid, 32 * t->warps, t->smem_wt, t->stream>>>(a);
+    const int grid = std::max(1, std::min(t->grid_wt, (t->n_wtiles + t->warps_wt - 1) / t->warps_wt));
+    dev::k_wt_build<true><<<grid, 32 * t->warps_wt, t->smem_wt, t->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     t->end_stage();
     return LDA_OK;
@@ -708,8 +722,8 @@ static dev::DtArgs dt_args(const lda_trainer* t, int chunk, int slot) {
 static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
     const dev::DtArgs a = dt_args(t, chunk, slot);
     const int64_t nd = a.d_end - a.d_begin;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps - 1) / t->warps));
-    dev::k_dt_build<<<grid, 32 * t->warps, t->smem_dt, q>>>(a);
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps_dt - 1) / t->warps_dt));
+    dev::k_dt_build<true><<<grid, 32 * t->warps_dt, t->smem_dt, q>>>(a);
     CUDA_TRY(cudaGetLastError());
     return LDA_OK;
 }
