@@ -195,6 +195,17 @@ int lda_trainer_iterate(lda_trainer* t, int32_t n_iters, int32_t ll_mode);
  * Document::GPU2CPU (EZLDA/Doc.cu:266-308) do around every sweep. */
 int lda_iterate_host(lda_trainer* t, const uint16_t* topics_in, uint16_t* topics_out,
                      int32_t ll_mode, double* ll_sum);
+/* lda_iterate_host without waiting, for a loop of sweeps through host buffers (the same
+ * per-chunk uploads and downloads, EZLDA/Doc.cu:266-308, overlapped across sweeps).  Both
+ * buffers must be pinned host memory (cudaHostAlloc / cudaHostRegister) and stay untouched
+ * until lda_trainer_wait returns.  When topics_in is the previous call's topics_out and
+ * nothing else ran on the trainer since, chunk c of it is uploaded as soon as the previous
+ * sweep has downloaded chunk c, while that sweep samples its later chunks.  No
+ * log-likelihood; not with stage timing on. */
+int lda_iterate_host_async(lda_trainer* t, const uint16_t* topics_in, uint16_t* topics_out);
+/* Waits for every sweep and copy enqueued on the trainer; reports a device error any of
+ * them found. */
+int lda_trainer_wait(lda_trainer* t);
 /* FP64 sum and token count of the last log-likelihood evaluation; EZLDA's
  * PerplexityKernel / LDATrainPerplexityReduce (EZLDA/SamplingKernel.cu:172-180,
  * profilePerp/utility.cu:2883-2925).  Mean per-token LL = ll_sum / n_tokens. */

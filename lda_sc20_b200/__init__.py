@@ -241,6 +241,16 @@ class Trainer:
         check(self._lib.lda_iterate_host(self._h, _ptr(z_in), _ptr(z_out), 1 if ll else 0, C.byref(out)))
         return out.value if ll else None
 
+    def iterate_host_async(self, z_in: np.ndarray, z_out: np.ndarray) -> None:
+        """One sweep through pinned host buffers without waiting (lda_iterate_host_async).
+        Keep both arrays alive and untouched until wait(); pass the previous call's z_out as
+        z_in to overlap each chunk's upload with the previous sweep."""
+        check(self._lib.lda_iterate_host_async(self._h, _ptr(z_in), _ptr(z_out)))
+
+    def wait(self) -> None:
+        """Waits for the sweeps and copies enqueued by iterate_host_async."""
+        check(self._lib.lda_trainer_wait(self._h))
+
     def loglik(self) -> tuple[float, int]:
         s, n = C.c_double(), C.c_int64()
         check(self._lib.lda_trainer_loglik(self._h, C.byref(s), C.byref(n)))

@@ -104,6 +104,8 @@ SIGNATURES = {
     "lda_trainer_topics_device": (I32, [P, C.POINTER(P), C.POINTER(I64)]),
     "lda_trainer_iterate": (I32, [P, I32, I32]),
     "lda_iterate_host": (I32, [P, P, P, I32, C.POINTER(F64)]),
+    "lda_iterate_host_async": (I32, [P, P, P]),
+    "lda_trainer_wait": (I32, [P]),
     "lda_trainer_loglik": (I32, [P, C.POINTER(F64), C.POINTER(I64)]),
     "lda_trainer_get_topics": (I32, [P, P, I64]),
     "lda_trainer_set_topics": (I32, [P, P, I64]),

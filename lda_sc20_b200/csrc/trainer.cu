@@ -120,6 +120,16 @@ struct lda_trainer {
     // chunk is sampled
     cudaStream_t copy_stream = nullptr;
     cudaEvent_t ev_chunk = nullptr, ev_copied = nullptr;
+    // asynchronous host-buffer sweeps (lda_iterate_host_async): uploads go on up_stream;
+    // ev_down[c] marks chunk c's download of the last such sweep into last_out, and
+    // last_seq the stage count right after it (nothing else enqueued since when equal)
+    cudaStream_t up_stream = nullptr;
+    cudaEvent_t ev_up = nullptr, ev_tail = nullptr;
+    std::vector<cudaEvent_t> ev_down;
+    bool record_down = false;
+    bool copies_pending = false;  // an asynchronous sweep's downloads may still read z
+    const uint16_t* last_out = nullptr;
+    uint64_t stage_seq = 0, last_seq = ~0ull;
     // resident sweeps without stage timing run chunk i of the range on work stream i mod 2,
     // so one chunk's doc-topic rebuild and sampling overlap the other's
     cudaStream_t work[2] = {nullptr, nullptr};
@@ -145,6 +155,13 @@ struct lda_trainer {
         }
         if (ev_chunk) cudaEventDestroy(ev_chunk);
         if (ev_copied) cudaEventDestroy(ev_copied);
+        if (up_stream) {
+            cudaStreamSynchronize(up_stream);
+            cudaStreamDestroy(up_stream);
+        }
+        if (ev_up) cudaEventDestroy(ev_up);
+        if (ev_tail) cudaEventDestroy(ev_tail);
+        for (cudaEvent_t e : ev_down) cudaEventDestroy(e);
         for (int i = 0; i < 2; ++i) {
             if (work[i]) {
                 cudaStreamSynchronize(work[i]);
@@ -182,6 +199,13 @@ struct lda_trainer {
     }
 
     EventPair* begin_stage(int stage) {
+        ++stage_seq;
+        if (copies_pending) {
+            // work that may write the topics comes after the downloads still reading them
+            cudaEventRecord(ev_copied, copy_stream);
+            cudaStreamWaitEvent(stream, ev_copied, 0);
+            copies_pending = false;
+        }
         if (!timing) return nullptr;
         EventPair e;
         if (!pool.empty()) { e = pool.back(); pool.pop_back(); }
@@ -875,6 +899,7 @@ static int copy_back(lda_trainer* t, int ch, cudaStream_t q, uint16_t* zout) {
     CUDA_TRY(cudaEventRecord(t->ev_chunk, q));
     CUDA_TRY(cudaStreamWaitEvent(t->copy_stream, t->ev_chunk, 0));
     CUDA_TRY(cudaMemcpyAsync(zout + t0, t->z + t0, sizeof(uint16_t) * (size_t)n, cudaMemcpyDeviceToHost, t->copy_stream));
+    if (t->record_down) CUDA_TRY(cudaEventRecord(t->ev_down[ch], t->copy_stream));
     return LDA_OK;
 }
 
@@ -1002,6 +1027,78 @@ extern "C" int lda_iterate_host(lda_trainer* t, const uint16_t* zin, uint16_t* z
     return LDA_OK;
 }
 
+static int make_host_copy_stream(lda_trainer* t) {
+    if (!t->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&t->copy_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_chunk, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_copied, cudaEventDisableTiming));
+    }
+    return LDA_OK;
+}
+
+extern "C" int lda_iterate_host_async(lda_trainer* t, const uint16_t* zin, uint16_t* zout) {
+    if (!t || !zin || !zout) return fail(LDA_ERR_ARG, "null argument");
+    if (zin == zout) return fail(LDA_ERR_ARG, "topics_in and topics_out must be different buffers");
+    if (t->timing) return fail(LDA_ERR_STATE, "stage timing is on (it serialises the stages); use lda_iterate_host");
+    CUDA_TRY(cudaSetDevice(t->device));
+    for (const void* p : {(const void*)zin, (const void*)zout}) {
+        cudaPointerAttributes pa{};
+        const bool pinned = cudaPointerGetAttributes(&pa, p) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (!pinned) return fail(LDA_ERR_ARG, "lda_iterate_host_async needs pinned host buffers (cudaHostAlloc / cudaHostRegister)");
+    }
+    int rc;
+    if ((rc = make_host_copy_stream(t))) return rc;
+    if (!t->up_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&t->up_stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_up, cudaEventDisableTiming));
+        CUDA_TRY(cudaEventCreateWithFlags(&t->ev_tail, cudaEventDisableTiming));
+        t->ev_down.assign(t->C, nullptr);
+        for (auto& e : t->ev_down) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    // Chained: topics_in is the previous asynchronous sweep's topics_out and nothing else
+    // was enqueued since.  Chunk c's upload then waits only for that sweep's download of
+    // chunk c (chunks read and write only their own tokens' topics; the word-topic rebuild,
+    // which reads them all, ran first).  Otherwise it waits for all enqueued work.
+    const bool chained = zin == t->last_out && t->stage_seq == t->last_seq;
+    if (!chained) {
+        CUDA_TRY(cudaEventRecord(t->ev_tail, t->stream));
+        CUDA_TRY(cudaStreamWaitEvent(t->up_stream, t->ev_tail, 0));
+        CUDA_TRY(cudaEventRecord(t->ev_copied, t->copy_stream));
+        CUDA_TRY(cudaStreamWaitEvent(t->up_stream, t->ev_copied, 0));
+    }
+    // topics outside the sampled chunk range come back unchanged
+    const int64_t r0 = t->chunk_tok[t->chunk_first], r1 = t->chunk_tok[t->chunk_last];
+    if (r0 > 0) std::memcpy(zout, zin, sizeof(uint16_t) * (size_t)r0);
+    if (r1 < t->N) std::memcpy(zout + r1, zin + r1, sizeof(uint16_t) * (size_t)(t->N - r1));
+    for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
+        const int64_t t0 = t->chunk_tok[ch], n = t->chunk_tok[ch + 1] - t0;
+        if (n <= 0) continue;
+        if (chained) CUDA_TRY(cudaStreamWaitEvent(t->up_stream, t->ev_down[ch], 0));
+        CUDA_TRY(cudaMemcpyAsync(t->z + t0, zin + t0, sizeof(uint16_t) * (size_t)n, cudaMemcpyHostToDevice, t->up_stream));
+    }
+    CUDA_TRY(cudaEventRecord(t->ev_up, t->up_stream));
+    CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_up, 0));
+    t->record_down = true;
+    rc = sweep_async(t, 0, zout);
+    t->record_down = false;
+    if (rc) return rc;
+    t->ll_valid = false;
+    t->last_out = zout;
+    t->last_seq = t->stage_seq;
+    t->copies_pending = true;
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_wait(lda_trainer* t) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    if (t->up_stream) CUDA_TRY(cudaStreamSynchronize(t->up_stream));
+    if (t->copy_stream) CUDA_TRY(cudaStreamSynchronize(t->copy_stream));
+    t->copies_pending = false;
+    return finish(t);
+}
+
 extern "C" int lda_trainer_loglik(lda_trainer* t, double* ll, int64_t* n) {
     if (!t || !ll) return fail(LDA_ERR_ARG, "null argument");
     if (!t->ll_valid) return fail(LDA_ERR_STATE, "no log-likelihood has been evaluated (run a sweep with ll_mode=1)");
@@ -1024,6 +1121,8 @@ extern "C" int lda_trainer_set_topics(lda_trainer* t, const uint16_t* in, int64_
         if (in[i] >= t->K) return fail(LDA_ERR_ARG, "topic %d of token %lld >= K=%d", in[i], (long long)i, t->K);
     CUDA_TRY(cudaSetDevice(t->device));
     CUDA_TRY(cudaStreamSynchronize(t->stream));
+    if (t->copy_stream) CUDA_TRY(cudaStreamSynchronize(t->copy_stream));
+    t->copies_pending = false;
     CUDA_TRY(cudaMemcpy(t->z, in, sizeof(uint16_t) * (size_t)count, cudaMemcpyHostToDevice));
     return LDA_OK;
 }

@@ -161,6 +161,42 @@ def test_host_iterate_matches_resident():
     assert np.array_equal(a.topics(), out)
 
 
+def test_async_host_sweeps_match_resident():
+    """lda_iterate_host_async chained through two pinned buffers (each chunk of the next
+    input goes up once the previous sweep has brought it down) equals resident sweeps; a
+    call after other work on the trainer takes the unchained path and equals the
+    synchronous host sweeps; pageable buffers are refused."""
+    import torch
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=4))
+    ref = L.Trainer(c, K=64)
+    tr = L.Trainer(c, K=64)
+    z0 = c.topics()
+    pin = lambda a: torch.from_numpy(a.view(np.int16).copy()).pin_memory()
+    p, q = pin(z0), pin(np.zeros_like(z0))
+    for _ in range(5):
+        tr.iterate_host_async(p.numpy().view(np.uint16), q.numpy().view(np.uint16))
+        p, q = q, p
+    tr.wait()
+    ref.iterate(5)
+    assert np.array_equal(p.numpy().view(np.uint16), ref.topics())
+    assert np.array_equal(tr.topics(), ref.topics())
+    # the same calls with other work in between: async, resident sweep, async again from
+    # the last output, against the synchronous host path
+    s1, s2 = L.Trainer(c, K=64), L.Trainer(c, K=64)
+    a1, b1 = pin(z0), pin(np.zeros_like(z0))
+    s1.iterate_host_async(a1.numpy().view(np.uint16), b1.numpy().view(np.uint16))
+    s1.iterate(1)
+    s1.iterate_host_async(b1.numpy().view(np.uint16), a1.numpy().view(np.uint16))
+    s1.wait()
+    o1, o2 = np.empty_like(z0), np.empty_like(z0)
+    s2.iterate_host(z0, o1)
+    s2.iterate(1)
+    s2.iterate_host(o1, o2)
+    assert np.array_equal(a1.numpy().view(np.uint16), o2)
+    with pytest.raises(L.LdaError):
+        s1.iterate_host_async(z0, np.empty_like(z0))
+
+
 def test_checkpoint_resume_is_exact(tmp_path):
     c = L.Corpus.generate(L.corpus_config("c0"))
     a = L.Trainer(c, K=64)
