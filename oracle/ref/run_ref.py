@@ -240,7 +240,7 @@ def mode_time(tmp, out, n=30):
     """EZLDA's per-sweep time (its own iterStart/iterStop events over its two-stream
     schedule, host<->device chunk copies included) against this library on the same
     corpus and sweeps: resident (lda_trainer_iterate) and through host buffers
-    (lda_iterate_host, topics uploaded and downloaded every sweep)."""
+    (lda_iterate_host_async, topics uploaded and downloaded chunk by chunk every sweep)."""
     import time as _time
     import torch
     c = make_corpus(REF_TIME)
@@ -272,8 +272,9 @@ def mode_time(tmp, out, n=30):
     tr.iteration = 0
     t0 = _time.perf_counter()
     for _ in range(n):
-        tr.iterate_host(a.numpy().view(np.uint16), b.numpy().view(np.uint16))
+        tr.iterate_host_async(a.numpy().view(np.uint16), b.numpy().view(np.uint16))
         a, b = b, a
+    tr.wait()
     e2e_ms = 1e3 * (_time.perf_counter() - t0) / n
     o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, ALPHA, BETA)
     ll_ref, ll_ours = oracle_ll(o, z_ref.astype(np.uint16)), oracle_ll(o, z_ours)
