@@ -130,6 +130,7 @@ struct lda_trainer {
     bool copies_pending = false;  // an asynchronous sweep's downloads may still read z
     const uint16_t* last_out = nullptr;
     uint64_t stage_seq = 0, last_seq = ~0ull;
+    int last_first = -1, last_last = -1;  // that sweep's chunk range
     // resident sweeps without stage timing run chunk i of the range on work stream i mod 2,
     // so one chunk's doc-topic rebuild and sampling overlap the other's
     cudaStream_t work[2] = {nullptr, nullptr};
@@ -1056,11 +1057,12 @@ extern "C" int lda_iterate_host_async(lda_trainer* t, const uint16_t* zin, uint1
         t->ev_down.assign(t->C, nullptr);
         for (auto& e : t->ev_down) CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    // Chained: topics_in is the previous asynchronous sweep's topics_out and nothing else
-    // was enqueued since.  Chunk c's upload then waits only for that sweep's download of
+    // Chained: topics_in is the previous asynchronous sweep's topics_out, over the same
+    // chunk range, and nothing else was enqueued since.  Chunk c's upload then waits only for that sweep's download of
     // chunk c (chunks read and write only their own tokens' topics; the word-topic rebuild,
     // which reads them all, ran first).  Otherwise it waits for all enqueued work.
-    const bool chained = zin == t->last_out && t->stage_seq == t->last_seq;
+    const bool chained = zin == t->last_out && t->stage_seq == t->last_seq && t->chunk_first == t->last_first &&
+                         t->chunk_last == t->last_last;
     if (!chained) {
         CUDA_TRY(cudaEventRecord(t->ev_tail, t->stream));
         CUDA_TRY(cudaStreamWaitEvent(t->up_stream, t->ev_tail, 0));
@@ -1086,6 +1088,8 @@ extern "C" int lda_iterate_host_async(lda_trainer* t, const uint16_t* zin, uint1
     t->ll_valid = false;
     t->last_out = zout;
     t->last_seq = t->stage_seq;
+    t->last_first = t->chunk_first;
+    t->last_last = t->chunk_last;
     t->copies_pending = true;
     return LDA_OK;
 }
