@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
         // phi_k = ((float)n_wk + beta) * r_k with r_k = 1 / ((float)n_k + V*beta), the values
         // fill_recip and build_column form
         for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
-            const float rk = __fdiv_rn(1.0f, fadd(__int2float_rn(__ldg(a.n_k + k)), a.Vbeta));
+            const float rk = a.recip ? __ldg(a.recip + k) : __fdiv_rn(1.0f, fadd(__int2float_rn(__ldg(a.n_k + k)), a.Vbeta));
             col[col_skew(k)] = fmul(fadd(__int2float_rn(__ldg(wrow + k)), a.beta), rk);
         }
         const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
@@ -464,6 +464,12 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
         for (uint32_t e = lane; e < nnz; e += 32) bits[(__ldg(ent + e) >> 16) >> 5] = 0u;
         __syncwarp();
     }
+}
+
+// r_k = 1 / ((float)n_k + V*beta), the value fill_recip forms, into a global table.
+__global__ void __launch_bounds__(256) k_recip(const int* __restrict__ n_k, int K, float Vbeta, float* r) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) r[k] = __fdiv_rn(1.0f, fadd(__int2float_rn(n_k[k]), Vbeta));
 }
 
 // Fixed-order FP64 reduction of the per-tile LL partials (one CTA of 1024 threads).

@@ -338,6 +338,9 @@ struct SampleArgs {
     // tok_doc / meta hold tokens [tok_base, ...) and dt_ent the doc-row entries
     // [dt_base, ...) (non-zero when the chunk is streamed into a slot buffer)
     uint32_t tok_base, dt_base;
+    // r_k = 1 / ((float)n_k + V*beta) for k < K, formed once per sweep (the K > kLargeK
+    // dense-word sampler reads it instead of dividing for every tile's column)
+    const float* recip = nullptr;
 };
 
 // Above this many topics the trainer samples with the CTA-per-tile dense-word kernel and

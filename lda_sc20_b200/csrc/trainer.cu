@@ -52,6 +52,7 @@ struct lda_trainer {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     int K = 0, Vd = 0, C = 0, warps = 8, num_sms = 0;
     int swarps = 8;  // warps per CTA of the K <= 2048 sampler
+    float* recip = nullptr;  // [K] per-sweep reciprocals (K > kLargeK)
     int warps_wt = 8, warps_dt = 8;  // warps per CTA of the word-topic and doc-topic rebuilds
     float alpha = 0, beta = 0, Vbeta = 0;
     uint64_t seed = 0;
@@ -454,7 +455,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
-                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + 2 * T.C, 4) + nb(kCounters, 8) +
+                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? nb(T.K, 4) : 0) +
                                  nb(1, 4);
         T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
     }
@@ -499,6 +500,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
     ALLOC(T.tile_ctr, 1 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
+    if (T.large) ALLOC(T.recip, T.K);
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
 
@@ -688,6 +690,9 @@ extern "C" int lda_max_topic(lda_trainer* t) {
             dev::k_word_stats_sparse_large<<<grid, 32 * kLargeWarps, t->smem_stats_sparse, t->stream>>>(a);
             CUDA_TRY(cudaGetLastError());
         }
+        // the sweep's reciprocals for the dense-word sampler's column builds
+        dev::k_recip<<<(t->K + 255) / 256, 256, 0, t->stream>>>(t->n_k, t->K, t->Vbeta, t->recip);
+        CUDA_TRY(cudaGetLastError());
     }
     t->end_stage();
     return LDA_OK;
@@ -768,6 +773,7 @@ static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, in
     a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.ctr = t->ctr;
     a.tok_base = b.tok_base;
     a.dt_base = b.dt_base;
+    a.recip = t->recip;
     return a;
 }
 
