@@ -195,6 +195,16 @@ def test_async_host_sweeps_match_resident():
     assert np.array_equal(a1.numpy().view(np.uint16), o2)
     with pytest.raises(L.LdaError):
         s1.iterate_host_async(z0, np.empty_like(z0))
+    # chunks streamed through two slot buffers take the same path
+    st = L.Trainer(c, K=64, stream_mode=2, num_streams=2)
+    p, q = pin(z0), pin(np.zeros_like(z0))
+    for _ in range(3):
+        st.iterate_host_async(p.numpy().view(np.uint16), q.numpy().view(np.uint16))
+        p, q = q, p
+    st.wait()
+    ref3 = L.Trainer(c, K=64)
+    ref3.iterate(3)
+    assert np.array_equal(p.numpy().view(np.uint16), ref3.topics())
 
 
 def test_checkpoint_resume_is_exact(tmp_path):
