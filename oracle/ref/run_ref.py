@@ -302,7 +302,7 @@ def _chi2_pvalue(h, p, n, chi2):
 
 
 def main():
-    out = sys.argv[1] if len(sys.argv) > 1 else "gpurun_out/ref"
+    out = sys.argv[1] if len(sys.argv) > 1 else "ref_out"
     modes = "counts,sweeps,dist"
     for a in sys.argv[2:]:
         if a.startswith("--modes="):
