@@ -1090,13 +1090,13 @@ extern "C" int lda_iterate_host_async(lda_trainer* t, const uint16_t* zin, uint1
     t->record_down = true;
     rc = sweep_async(t, 0, zout);
     t->record_down = false;
+    t->copies_pending = true;  // also on failure: some downloads may be enqueued
     if (rc) return rc;
     t->ll_valid = false;
     t->last_out = zout;
     t->last_seq = t->stage_seq;
     t->last_first = t->chunk_first;
     t->last_last = t->chunk_last;
-    t->copies_pending = true;
     return LDA_OK;
 }
 
