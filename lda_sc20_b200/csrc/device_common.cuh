@@ -292,41 +292,51 @@ struct ColShared {
     __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
 };
 
-// Serial per-lane sum over the lane's block [b0, b1) of a doc row (one fmaf chain; the
-// loads of two entries are issued together).
+// Serial per-lane sum over the lane's entries l, l + 32, l + 64, ... of a doc row of nnz
+// entries (one fmaf chain).  A warp's loads of one step then read 32 consecutive entries,
+// one or two 128-byte lines, where contiguous per-lane blocks would touch one line per
+// lane block.  The loads of two steps are issued together.
 template <class View>
-__device__ __forceinline__ float block_mass(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
-                                            const View& colz) {
+__device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uint32_t lane, uint32_t nnz,
+                                           const View& colz) {
     float acc = 0.0f;
-    uint32_t q = b0;
-    for (; q + 2 <= b1; q += 2) {
-        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 1);
+    uint32_t q = lane;
+    for (; q + 32u < nnz; q += 64u) {
+        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
         acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
         acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
     }
-    if (q < b1) {
+    if (q < nnz) {
         const uint32_t e = __ldg(row + q);
         acc = ffma(u2f(e & 0xffffu), colz((int)(e >> 16)), acc);
     }
     return acc;
 }
 
-// The S-bucket draw inside one lane block: the block's serial partial sums (the same
-// fmaf chain as block_mass) are compared with t2; the first entry with colz > 0 whose
-// partial sum exceeds t2 wins, else the last entry with colz > 0, else `fallback`.
+// The S-bucket draw among lane ls's entries ls, ls + 32, ... of the row: their serial
+// partial sums (the fmaf chain of lane_mass) are compared with t2; the first entry with
+// colz > 0 whose partial sum exceeds t2 wins, else the last entry with colz > 0, else
+// `fallback`.  Each entry of the lane sits on its own 128-byte line, so the loads of four
+// entries are issued before any of them is used.
 template <class View>
-__device__ __forceinline__ int block_draw(const uint32_t* __restrict__ row, uint32_t b0, uint32_t b1,
-                                          const View& colz, float t2, int fallback) {
+__device__ __forceinline__ int lane_draw(const uint32_t* __restrict__ row, uint32_t ls, uint32_t nnz,
+                                         const View& colz, float t2, int fallback) {
     float acc = 0.0f;
     int last = -1;
-    for (uint32_t q = b0; q < b1; ++q) {
-        const uint32_t e = __ldg(row + q);
-        const int k = (int)(e >> 16);
-        const float cz = colz(k);
-        acc = ffma(u2f(e & 0xffffu), cz, acc);
-        if (cz > 0.0f) {
-            last = k;
-            if (t2 < acc) return k;
+    for (uint32_t q = ls; q < nnz; q += 128u) {
+        uint32_t e[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) e[s] = q + 32u * s < nnz ? __ldg(row + q + 32u * s) : 0u;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (q + 32u * s >= nnz) break;
+            const int k = (int)(e[s] >> 16);
+            const float cz = colz(k);
+            acc = ffma(u2f(e[s] & 0xffffu), cz, acc);
+            if (cz > 0.0f) {
+                last = k;
+                if (t2 < acc) return k;
+            }
         }
     }
     return last >= 0 ? last : fallback;

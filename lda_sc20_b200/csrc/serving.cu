@@ -113,14 +113,15 @@ __device__ __forceinline__ float colz_of(const float* __restrict__ prow, int mk,
     return (int)k == mk ? 0.0f : __ldg(prow + k);
 }
 
-// Serial fmaf chain over entries [b0, b1) of the document row with phi gathered from the
-// frozen matrix; the gathers of four entries are issued before their products are summed.
-__device__ __forceinline__ float fold_block_mass(const uint32_t* row, uint32_t b0, uint32_t b1,
-                                                 const float* __restrict__ prow, int mk) {
+// Serial fmaf chain over the lane's entries l, l + 32, ... of the document row (in shared
+// memory, so a step's 32 reads are conflict-free) with phi gathered from the frozen
+// matrix; the gathers of four entries are issued before their products are summed.
+__device__ __forceinline__ float fold_lane_mass(const uint32_t* row, uint32_t lane, uint32_t nnz,
+                                                const float* __restrict__ prow, int mk) {
     float acc = 0.0f;
-    uint32_t q = b0;
-    for (; q + 4 <= b1; q += 4) {
-        const uint32_t e0 = row[q], e1 = row[q + 1], e2 = row[q + 2], e3 = row[q + 3];
+    uint32_t q = lane;
+    for (; q + 96u < nnz; q += 128u) {
+        const uint32_t e0 = row[q], e1 = row[q + 32u], e2 = row[q + 64u], e3 = row[q + 96u];
         const float c0 = colz_of(prow, mk, e0 >> 16), c1 = colz_of(prow, mk, e1 >> 16);
         const float c2 = colz_of(prow, mk, e2 >> 16), c3 = colz_of(prow, mk, e3 >> 16);
         acc = ffma(u2f(e0 & 0xffffu), c0, acc);
@@ -128,27 +129,27 @@ __device__ __forceinline__ float fold_block_mass(const uint32_t* row, uint32_t b
         acc = ffma(u2f(e2 & 0xffffu), c2, acc);
         acc = ffma(u2f(e3 & 0xffffu), c3, acc);
     }
-    for (; q < b1; ++q) {
+    for (; q < nnz; q += 32u) {
         const uint32_t e = row[q];
         acc = ffma(u2f(e & 0xffffu), colz_of(prow, mk, e >> 16), acc);
     }
     return acc;
 }
 
-// The S-bucket draw inside one lane block (the partial sums of fold_block_mass): the first
-// entry with colz > 0 whose partial sum exceeds t2, else the last entry with colz > 0,
-// else mk.
-__device__ __forceinline__ int fold_block_draw(const uint32_t* row, uint32_t b0, uint32_t b1,
-                                               const float* __restrict__ prow, int mk, float t2) {
+// The S-bucket draw among lane ls's entries ls, ls + 32, ... (the partial sums of
+// fold_lane_mass): the first entry with colz > 0 whose partial sum exceeds t2, else the
+// last entry with colz > 0, else mk.
+__device__ __forceinline__ int fold_lane_draw(const uint32_t* row, uint32_t ls, uint32_t nnz,
+                                              const float* __restrict__ prow, int mk, float t2) {
     float acc = 0.0f;
     int last = -1;
-    uint32_t q = b0;
-    for (; q + 4 <= b1; q += 4) {
+    uint32_t q = ls;
+    for (; q + 96u < nnz; q += 128u) {
         uint32_t e[4];
         float c[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            e[j] = row[q + j];
+            e[j] = row[q + 32u * j];
             c[j] = colz_of(prow, mk, e[j] >> 16);
         }
 #pragma unroll
@@ -160,7 +161,7 @@ __device__ __forceinline__ int fold_block_draw(const uint32_t* row, uint32_t b0,
             }
         }
     }
-    for (; q < b1; ++q) {
+    for (; q < nnz; q += 32u) {
         const uint32_t e = row[q];
         const float cz = colz_of(prow, mk, e >> 16);
         acc = ffma(u2f(e & 0xffffu), cz, acc);
@@ -230,7 +231,6 @@ __global__ void __launch_bounds__(256) k_foldin(FoldArgs a) {
             nnz += (uint32_t)__popc(bal);
         }
         __syncwarp();
-        const uint32_t B = (nnz + 31u) >> 5;
         uint32_t cur_w = 0xffffffffu;
         float SL = 0.0f, SP = 0.0f, S = 0.0f;
         const uint32_t end = min(begin + a.item_tokens, len);
@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(256) k_foldin(FoldArgs a) {
             }
             int znew = mk;
             bool defer = false;
-            uint32_t my_b0 = 0, my_b1 = 0;
+            uint32_t my_ls = 0;
             float my_t2 = 0.0f;
             unsigned need = __ballot_sync(FULL, valid && !ea);
             while (need) {
@@ -269,8 +269,7 @@ __global__ void __launch_bounds__(256) k_foldin(FoldArgs a) {
                 const float* prow = a.phi + (size_t)wj * a.K;
                 if (wj != cur_w) {
                     cur_w = wj;
-                    const uint32_t b0 = min(lane * B, nnz), b1 = min(b0 + B, nnz);
-                    SL = fold_block_mass(row, b0, b1, prow, mkj);
+                    SL = fold_lane_mass(row, (uint32_t)lane, nnz, prow, mkj);
                     SP = warp_ks_scan(SL, lane);
                     S = __shfl_sync(FULL, SP, 31);
                 }
@@ -287,8 +286,7 @@ __global__ void __launch_bounds__(256) k_foldin(FoldArgs a) {
                     const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
                     if (lane == j) {
                         defer = true;
-                        my_b0 = (uint32_t)ls * B;
-                        my_b1 = min(my_b0 + B, nnz);
+                        my_ls = (uint32_t)ls;
                         my_t2 = ls > 0 ? fsub(tt, prev) : tt;
                     }
                 } else {
@@ -313,7 +311,7 @@ __global__ void __launch_bounds__(256) k_foldin(FoldArgs a) {
                     if (lane == j) znew = zq;
                 }
             }
-            if (defer) znew = fold_block_draw(row, my_b0, my_b1, a.phi + (size_t)w * a.K, mk, my_t2);
+            if (defer) znew = fold_lane_draw(row, my_ls, nnz, a.phi + (size_t)w * a.K, mk, my_t2);
             if (valid) zout[off + pos] = (uint16_t)znew;
         }
         __syncwarp();

@@ -298,12 +298,12 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& his
 // warp-private shared memory.  Each 32-token group is screened thread-per-token by the
 // max-topic bound.  Tokens the bound does not settle (all tokens in LL mode) are then
 // evaluated one at a time by the whole warp, with uniform control flow:
-//   S      lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
-//          one Kogge-Stone scan gives the lane prefixes; a doc row is evaluated once
-//          for consecutive tokens of the same (word, doc) in the tile;
-//   bucket a ballot over the lane prefixes picks the block of an S-bucket draw; the
-//          in-block draw (at most B entries) runs afterwards thread-per-token, all the
-//          group's S-bucket tokens at once;
+//   S      lane l sums the doc row's entries l, l+32, l+64, ... (coalesced loads); one
+//          Kogge-Stone scan gives the lane prefixes; a doc row is evaluated once for
+//          consecutive tokens of the same (word, doc) in the tile;
+//   bucket a ballot over the lane prefixes picks the lane of an S-bucket draw; the
+//          in-lane draw (at most ceil(nnz/32) entries) runs afterwards thread-per-token,
+//          all the group's S-bucket tokens at once;
 //   Q      a ballot over the per-word lane prefixes of Q, then one topic per lane with a
 //          scan and a ballot (topics k = l, l+32, ..., 32 per round, carried).
 // Replaces UpdateProbKernelTrainD1, LDAKernelTrainD and LDAKernelTrain
@@ -384,7 +384,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                                                 float QP, float Q, const View& colz, uint32_t* ctr, int lane,
                                                 const float2* qtab = nullptr, int qrounds = 0) {
     double ll = 0.0;
-    uint32_t cur = 0xffffffffu, nnz = 0, B = 0;
+    uint32_t cur = 0xffffffffu, nnz = 0;
     const uint32_t* row = a.dt_ent;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
     for (uint32_t g = g0; g < cnt; g += gstep) {
@@ -409,7 +409,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
         int znew = maxK;
         // per-lane record of this token's evaluation, for the deferred draw and counters
         const uint32_t* my_row = row;
-        uint32_t my_b0 = 0, my_b1 = 0;
+        uint32_t my_ls = 0, my_nnz_s = 0;
         float my_t2 = 0.0f, my_total = 0.0f;
         int kind = BR_NONE;
         bool evaluated = false;
@@ -425,9 +425,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 cur = dj;
                 nnz = __shfl_sync(FULL, my_nnz, j);
                 row = a.dt_ent + __shfl_sync(FULL, my_off, j);
-                B = (nnz + 31u) >> 5;
-                const uint32_t b0 = min(lane * B, nnz);
-                SL = block_mass(row, b0, min(b0 + B, nnz), colz);
+                SL = lane_mass(row, (uint32_t)lane, nnz, colz);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
                 evaluated |= (lane == j);
@@ -450,8 +448,8 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 if (lane == j) {
                     kind = BR_S;
                     my_row = row;
-                    my_b0 = (uint32_t)ls * B;
-                    my_b1 = min(my_b0 + B, nnz);
+                    my_ls = (uint32_t)ls;
+                    my_nnz_s = nnz;
                     my_t2 = ls > 0 ? fsub(tt, prev) : tt;
                 }
             } else {
@@ -482,7 +480,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
         // each lane's own token's log-likelihood term, all lanes at once (every lane
         // accumulates only its own tokens, in group order)
         if (LL && valid) ll += log((double)my_total / ((double)nd + a.den_add));
-        if (kind == BR_S) znew = block_draw(my_row, my_b0, my_b1, colz, my_t2, maxK);
+        if (kind == BR_S) znew = lane_draw(my_row, my_ls, my_nnz_s, colz, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
         const bool in_need = (need0 >> lane) & 1u;

@@ -60,6 +60,7 @@ def lib() -> C.CDLL:
         L.orc_foldin_init.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_int32]
         L.orc_foldin_init.restype = C.c_uint16
         L.orc_get_phi_row.argtypes = [P, C.c_int32, P]
+        L.orc_set_doc_range.argtypes = [P, C.c_int32, C.c_int32]
         _lib = L
     return _lib
 
@@ -170,6 +171,11 @@ class Oracle:
         if rc:
             raise ValueError(f"orc_iterate failed ({rc})")
         return st
+
+    def set_doc_range(self, d0: int, d1: int) -> None:
+        """Sample only the tokens of docs [d0, d1) from now on (the default is all)."""
+        if lib().orc_set_doc_range(self._h, d0, d1):
+            raise ValueError(f"bad doc range [{d0}, {d1})")
 
     def token_probs(self, tok: int):
         p = np.empty(self.K, dtype=np.float64)

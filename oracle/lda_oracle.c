@@ -35,12 +35,12 @@
  *   shat    = fmaf((float)c2, phi_2nd, (float)rest * phi_3rd)
  *   bound   = (pmax + shat) + Q;   early accept  <=>  u*bound < pmax
  *   colz    = phi with colz[maxK] = 0
- *   B       = ceil(nnz / 32); SL[l] = serial fmaf((float)cnt_e, colz[k_e], acc)
- *             over the row entries e in [l*B, min(l*B+B, nnz)) (row ascending in k)
+ *   SL[l]   = serial fmaf((float)cnt_e, colz[k_e], acc) over the row entries
+ *             e = l, l+32, l+64, ... < nnz (row ascending in k)
  *   SP      = Kogge-Stone scan of SL; S = SP[31]
  *   pS      = pmax + S; total = pS + Q; target = u*total
  *   target < pmax -> maxK;
- *   target < pS   -> S bucket, t = target - pmax, lanes (SL, SP); in block l the
+ *   target < pS   -> S bucket, t = target - pmax, lanes (SL, SP); in lane l the
  *                    serial partial sums of SL[l]'s fmaf chain are compared with t2;
  *   otherwise     -> Q bucket, t = target - pS, lanes (QL, QP), slots of lane l:
  *                    k = l, l+32, ... < K, term = alpha * colz[k], in rounds of 32
@@ -100,6 +100,7 @@ uint16_t orc_init_topic(uint64_t seed, uint64_t tok, int32_t K) {
 /* ------------------------------------------------------------------- state */
 struct orc_state {
     int64_t N;
+    int32_t doc_lo, doc_hi; /* orc_sample draws only tokens of docs in [doc_lo, doc_hi) */
     int32_t V, D, K, nthreads;
     float alpha, beta;
     const int32_t* tok_word;
@@ -150,6 +151,7 @@ orc_state* orc_create(int64_t N, int32_t V, int32_t D, int32_t K, const int32_t*
     s->nthreads = nthreads > 0 ? nthreads : 1;
     s->alpha = alpha; s->beta = beta;
     s->tok_word = tok_word; s->tok_doc = tok_doc;
+    s->doc_lo = 0; s->doc_hi = D;
     s->woff = counting_index(N, V, tok_word, &s->wtok);
     s->doff = counting_index(N, D, tok_doc, &s->dtok);
     s->rcap = (int64_t*)calloc((size_t)D + 1, sizeof(int64_t));
@@ -512,14 +514,13 @@ static int32_t draw_token(const word_ctx* w, const uint32_t* row, int32_t nnz, i
     *total_out = 0.0f;
     *branch = BR_MAX;
     if (ea && !force_eval) return w->maxK;
-    /* S: lane l sums the contiguous block [l*B, l*B+B) of the doc row, B = ceil(nnz/32);
-     * the lane sums are Kogge-Stone scanned (EZLDA sums the same row in 32-entry blocks,
-     * EZLDA/utility.cu:1376-1440) */
-    const int32_t B = (nnz + LANES - 1) / LANES;
+    /* S: lane l sums the doc row's entries l, l+32, l+64, ...; the lane sums are
+     * Kogge-Stone scanned (EZLDA likewise strides the row over a warp's lanes in 32-entry
+     * steps, EZLDA/utility.cu:1376-1440) */
     float SL[LANES], SP[LANES];
     for (int l = 0; l < LANES; ++l) {
         float acc = 0.0f;
-        for (int32_t q = l * B; q < l * B + B && q < nnz; ++q)
+        for (int32_t q = l; q < nnz; q += LANES)
             acc = fmaf((float)(row[q] & 0xffffu), w->colz[row[q] >> 16], acc);
         SL[l] = acc;
     }
@@ -538,10 +539,10 @@ static int32_t draw_token(const word_ctx* w, const uint32_t* row, int32_t nnz, i
         const int l = pick_lane(tt, SP, SL);
         const float t2 = tt - (l > 0 ? SP[l - 1] : 0.0f);
         if (l < 0) return w->maxK;
-        /* the block's serial partial sums (the fmaf chain of SL[l]) */
+        /* the lane's serial partial sums (the fmaf chain of SL[l]) */
         float acc = 0.0f;
         int32_t last = -1;
-        for (int32_t q = l * B; q < l * B + B && q < nnz; ++q) {
+        for (int32_t q = l; q < nnz; q += LANES) {
             const int32_t k = (int32_t)(row[q] >> 16);
             acc = fmaf((float)(row[q] & 0xffffu), w->colz[k], acc);
             if (w->colz[k] > 0.0f) {
@@ -612,6 +613,7 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
         for (int64_t j = s->woff[w]; j < s->woff[w + 1]; ++j) {
             const int64_t t = s->wtok[j];
             const int32_t d = s->tok_doc[t];
+            if (d < s->doc_lo || d >= s->doc_hi) continue;
             const int32_t nd = (int32_t)(s->doff[d + 1] - s->doff[d]);
             const uint32_t* row = s->rent + s->rcap[d];
             const int32_t nnz = s->rnnz[d];
@@ -668,6 +670,13 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
     for (int32_t w = 0; w < s->V; ++w) tot.loglik += x.wll[w];
     free(x.icnt); free(x.fcol); free(x.part); free(x.wll);
     if (st) *st = tot;
+    return 0;
+}
+
+int orc_set_doc_range(orc_state* s, int32_t d0, int32_t d1) {
+    if (!s || d0 < 0 || d1 < d0 || d1 > s->D) return -1;
+    s->doc_lo = d0;
+    s->doc_hi = d1;
     return 0;
 }
 

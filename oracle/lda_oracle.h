@@ -79,6 +79,11 @@ typedef struct {
 int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter,
                int32_t ll_mode, int32_t word_stride, orc_sample_stats* st);
 
+/* Restricts orc_sample / orc_iterate to the tokens of docs [d0, d1) (the documents of a
+ * range of chunks: what one rank of a document-sharded sweep samples); the others keep
+ * their topics.  The default is every document. */
+int orc_set_doc_range(orc_state* s, int32_t d0, int32_t d1);
+
 /* Rebuild + sample: one full iteration, z updated in place. */
 int orc_iterate(orc_state* s, uint16_t* z, uint64_t seed, uint32_t iter,
                 int32_t ll_mode, orc_sample_stats* st);
