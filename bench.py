@@ -15,7 +15,18 @@ the topics are then reset), so the number is the average over a training run, ea
 
 --impl reference times the CPU restatement of the reference's sweep on the host cores.
 EZLDA has no CPU implementation of its sampler, so that arm runs the oracle port
-(oracle/liblda_oracle.c) with all host threads on a bounded sample of the same workload.
+(oracle/liblda_oracle.c) with all host threads.  Its step is one whole sweep (count
+rebuild + sampling of every token) of a bounded sample of the workload: 1/50 of the
+documents drawn from the same generative process by a numpy generator
+(oracle/sample_corpus.py), so that arm never loads the product library.  The cpu_baseline
+leg of the default run uses the same definition (same sample, same sweeps).
+
+Reference legs of the default run (baselines, never on the measured path):
+  cpu_baseline   the oracle port as above;
+  ezlda_b200     EZLDA's own kernels (oracle/_ref/ref_harness, built from the reference's
+                 sources) timed on this B200 with their own events, against this library on
+                 the same corpus, when the harness binary is present;
+  serving        the fold-in serving figures (one at a time, saturated batch, offered loads).
 """
 from __future__ import annotations
 
@@ -41,7 +52,6 @@ WORKLOADS = {
            "topics, Zipf(1.05) phi base (urn form), K=10000, alpha=0.1, beta=0.01, top-20000 dense "
            "words, 8 chunks; sweeps 0..K-1 from random initial topics"),
 }
-WORKLOAD = WORKLOADS["c1"]
 ALPHA = {"c2": 0.1, "c2s": 0.1}  # other presets: 50/K
 
 
@@ -60,7 +70,8 @@ def parse_args():
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--cpu-word-stride", type=int, default=40)
+    p.add_argument("--no-ezlda", action="store_true", help="skip the EZLDA-on-this-GPU reference leg")
+    p.add_argument("--no-serving", action="store_true", help="skip the fold-in serving figures")
     p.add_argument("--preset", default="c1")
     p.add_argument("--chunks", type=int, default=0, help="override the preset's chunk count")
     p.add_argument("--sharded", action="store_true",
@@ -279,10 +290,8 @@ def run_sharded(args, world, rank, local):
             "metric": METRIC, "value": N * args.steps / (ms / 1e3), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload(args.preset), "tokens": N, "docs": info.num_docs, "vocab": info.vocab, "K": K,
-                       "dense_words": info.num_dense, "chunks": info.num_chunks,
-                       "l2": "inputs_larger_than_l2 (resident corpus ~1.6 GB per sweep pass)",
-                       "parallelism": f"doc-sharded x{world}: chunks {st.ranges}, NCCL topic broadcast per sweep"},
+            "config": workload_config(args.preset, args.chunks), "tokens_per_step": N, "dense_words": info.num_dense,
+            "run": {"parallelism": f"doc-sharded x{world}: chunks {st.ranges}, NCCL topic exchange per sweep"},
             "loglik_per_token": ll_mean, "ranks_agree": agree, "e2e": e2e,
             "gpu_launches": tm.launches_wt + tm.launches_stats + tm.launches_dt + tm.launches_sample + tm.launches_ll,
             "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -363,6 +372,8 @@ def run_ours(args, world, rank, local):
     cnt = tr.counters()
     tr.set_timing(False)
     ms_staged = tm.ms_wt + tm.ms_stats + tm.ms_dt + tm.ms_sample
+    device_bytes = tr.device_bytes
+    streamed_gib = tr.stream_info()[2] / 2**30
     # log-likelihood of the state after the K timed sweeps (one extra evaluation sweep)
     z_after = tr.topics()
     ll_mean = tr.iterate(1, ll=True)
@@ -432,26 +443,44 @@ def run_ours(args, world, rank, local):
         e2e = {"value": world * N * sweeps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": 2 * N,
                "d2h_bytes_per_step": 2 * N, "ms_per_step": 1e3 * e2e_s / sweeps}
 
+    # fold-in serving against this corpus' model after 100 sweeps (the serving workload's
+    # frozen word-topic counts)
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving and args.preset == "c1" and not streaming:
+        from lda_sc20_b200.serving import Model
+        tr.set_topics(z0)
+        tr.iteration = 0
+        tr.iterate(100)
+        model = Model(tr)
+        serving = serving_figures(model, corpus, args.serve_sweeps, args.serve_rates, args.serve_seconds)
+        model.close()
+    tm_launches = tm.launches_wt + tm.launches_stats + tm.launches_dt + tm.launches_sample + tm.launches_ll
+    tr.close()
+
+    # reference legs (baselines; rank 0 of a one-GPU run only)
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(corpus, tr, z0, K, sweeps, args.cpu_word_stride)
+    ezlda = None
+    if rank == 0 and world == 1:
+        if not args.no_cpu_baseline:
+            c = cpu_sweeps(args.preset, args.warmup, sweeps)
+            cpu = {k: c[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        if not args.no_ezlda and K == 1024:
+            ezlda = ezlda_leg()
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": sweeps,
             "warmup": args.warmup, "ms_per_step": ms / sweeps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload(args.preset), "tokens": N, "docs": info.num_docs, "vocab": info.vocab,
-                       "K": K, "alpha": tr.alpha, "dense_words": info.num_dense, "chunks": info.num_chunks,
-                       "l2": "inputs_larger_than_l2 (the corpus pass per sweep exceeds the 126 MB L2)",
-                       "parallelism": "single GPU",
-                       "chunks_streamed": (f"{n_streams} streams, {tr.stream_info()[2] / 2**30:.1f} GiB "
-                                           f"copied host->device in total") if streaming else "no (resident)",
-                       "device_bytes": tr.device_bytes},
+            "config": workload_config(args.preset, args.chunks),
+            "tokens_per_step": N, "dense_words": info.num_dense,
+            "run": {"parallelism": "single GPU", "device_bytes": device_bytes,
+                    "chunks_streamed": (f"{n_streams} streams, {streamed_gib:.1f} GiB copied host->device in total")
+                    if streaming else "no (resident)"},
             "loglik_per_token": ll_mean,
             "ms_per_step_with_ll": ms_ll_sweep,
             "e2e": e2e,
-            "gpu_launches": tm.launches_wt + tm.launches_stats + tm.launches_dt + tm.launches_sample + tm.launches_ll,
+            "gpu_launches": tm_launches,
             "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
@@ -473,9 +502,10 @@ def run_ours(args, world, rank, local):
                                "branch_max": cnt.branch_max, "branch_s": cnt.branch_s, "branch_q": cnt.branch_q},
             "clocks": clk,
             "cpu_baseline": cpu,
+            "ezlda_b200": ezlda,
+            "serving": serving,
         }
         print(json.dumps(line), flush=True)
-    tr.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -486,101 +516,82 @@ def check_iter(tr, n):
     tr.iterate(n)
 
 
-def cpu_baseline(corpus, tr, z0, K, sweeps, stride):
-    """Oracle port on the host cores at the training state of sweep K/2 (a representative
-    mid-run state): full count rebuild plus sampling of every `stride`-th word."""
+CPU_SAMPLE_DOC_FRACTION = 50  # the CPU legs sweep 1/50 of the preset's documents
+
+
+def cpu_sweeps(preset: str, warmup: int, steps: int) -> dict:
+    """The CPU leg: the oracle port, all host threads, timing whole sweeps (count rebuild +
+    sampling of every token) of a sample corpus of 1/50 of the preset's documents, drawn
+    from the same generative process.  `warmup` untimed sweeps, then `steps` timed ones
+    from the sample's random initial topics (the same sweep indices the GPU arm times).
+    Loads only the oracle library."""
     import numpy as np
+    import lda_sc20_b200 as L  # presets only (pure Python; the native library is not loaded)
     from oracle import Oracle
-    tr.set_topics(z0)
-    tr.iteration = 0
-    tr.iterate(sweeps // 2)
-    zmid = tr.topics()
-    info = corpus.info
+    from oracle.sample_corpus import draw_corpus
+    cfg = L.corpus_config(preset)
+    D = max(1, cfg.num_docs // CPU_SAMPLE_DOC_FRACTION)
+    c = draw_corpus(cfg, D, seed=int(cfg.corpus_seed) + 7)
+    K = c["K"]
+    alpha = ALPHA.get(preset, 50.0 / K)
     nt = os.cpu_count() or 1
-    o = Oracle(corpus.tok_word(), corpus.tok_doc(), info.vocab, info.num_docs, K, tr.alpha, tr.beta, nthreads=nt)
-    t0 = time.perf_counter()
-    o.rebuild(zmid)
-    t1 = time.perf_counter()
-    zz = zmid.copy()
-    st = o.sample(zz, 42, sweeps // 2, word_stride=stride)
-    t2 = time.perf_counter()
-    N = info.num_tokens
-    per_sweep = (t1 - t0) + (t2 - t1) * N / max(st.tokens, 1)
-    g = tr.topics()
-    sel = (corpus.tok_word() % stride) == 0
-    tr.set_topics(zmid)
-    tr.iteration = sweeps // 2
-    tr.iterate(1)
-    agree = bool(np.array_equal(tr.topics()[sel], zz[sel]))
-    del g
-    return {"value": N / per_sweep, "unit": UNIT, "cores": nt, "kind": "port",
-            "sample": (f"state after sweep {sweeps // 2}: full rebuild of all counts ({t1 - t0:.2f} s) + "
-                       f"sampling every {stride}th word ({st.tokens} of {N} tokens, {t2 - t1:.2f} s), "
-                       f"extrapolated to one sweep; GPU agrees token-for-token on the sample: {agree}")}
+    o = Oracle(c["tok_word"], c["tok_doc"], c["V"], c["D"], K, alpha, 0.01, nthreads=nt)
+    z = c["topics"].copy()
+    for it in range(warmup):
+        o.iterate(z, 42, it)
+    times = []
+    for it in range(warmup, warmup + steps):
+        t0 = time.perf_counter()
+        o.iterate(z, 42, it)
+        times.append(time.perf_counter() - t0)
+    sec = float(np.mean(times))
+    N = c["N"]
+    return {"value": N / sec, "unit": UNIT, "cores": nt, "kind": "port", "ms_per_step": 1e3 * sec,
+            "tokens_per_step": N,
+            "sample": (f"whole sweeps (rebuild + sampling of every token) of a {D}-document, {N}-token corpus "
+                       f"drawn by oracle/sample_corpus.py from the preset's generative process (1/"
+                       f"{CPU_SAMPLE_DOC_FRACTION} of its documents); sweeps {warmup}..{warmup + steps - 1} "
+                       f"after {warmup} untimed ones; {nt} threads; per-sweep seconds min/median/max "
+                       f"{min(times):.3f}/{float(np.median(times)):.3f}/{max(times):.3f}")}
+
+
+def workload_config(preset: str, chunks: int = 0) -> dict:
+    """The workload both arms name: the preset's generator parameters (pure Python, no
+    native library)."""
+    import lda_sc20_b200 as L
+    g = L.corpus_config(preset)
+    return {"workload": workload(preset), "docs": int(g.num_docs), "vocab": int(g.vocab), "K": int(g.K),
+            "alpha": float(ALPHA.get(preset, 50.0 / g.K)), "beta": 0.01, "corpus_seed": int(g.corpus_seed),
+            "chunks": int(chunks or g.num_chunks),
+            "l2": "inputs_larger_than_l2 (one sweep passes over the resident corpus, >1 GB, against a 126 MB L2)"}
 
 
 def run_reference(args, world, rank, local):
-    """CPU restatement of the reference sweep (oracle port), all host threads."""
+    """CPU restatement of the reference sweep (oracle port), all host threads, rank 0 only."""
     if rank != 0:
         return
-    from oracle import Oracle
-    corpus = make_corpus(args.preset, 0)
-    info = corpus.info
-    K = info.K_hint
-    N = info.num_tokens
-    nt = os.cpu_count() or 1
-    alpha, beta = 50.0 / K, 0.01
-    o = Oracle(corpus.tok_word(), corpus.tok_doc(), info.vocab, info.num_docs, K, alpha, beta, nthreads=nt)
-    z = corpus.topics()
-    t0 = time.perf_counter()
-    o.rebuild(z)
-    t_rebuild = time.perf_counter() - t0
-    stride = max(1, args.cpu_word_stride * 10)
-    times, toks = [], 0
-    for s in range(args.warmup + args.steps):
-        zz = z.copy()
-        t1 = time.perf_counter()
-        st = o.sample(zz, 42, 0, word_stride=stride)
-        dt = time.perf_counter() - t1
-        if s >= args.warmup:
-            times.append(dt)
-            toks = st.tokens
-    per_sweep = t_rebuild + statistics.mean(times) * N / max(toks, 1)
-    value = N / per_sweep
-    sample = (f"sweep 0 state: full count rebuild ({t_rebuild:.2f} s, once) + per step sampling of every "
-              f"{stride}th word ({toks} of {N} tokens), extrapolated to one sweep; {nt} threads")
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * per_sweep, "higher_is_better": True,
+    cpu = cpu_sweeps(args.preset, args.warmup, args.steps)
+    line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"], "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "tokens": N, "K": K}, "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port", "sample": sample},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": workload_config(args.preset, args.chunks), "impl": "reference",
+            "tokens_per_step": cpu["tokens_per_step"],
+            "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args, local):
-    """Fold-in serving against the word side of the K=1024 corpus trained for 100 sweeps.
-
-    Requests are new documents from the corpus' generative process (its topic-word
-    distributions, fresh theta), lengths lognormal(median 150, sigma 1.0) clipped to
-    [5, 4000]; each runs the configured sweeps (default 30) and returns theta as FP32[K].
-    Measured: one request at a time (max_active=1, closed loop), a saturated batch (all
-    requests queued at once), and real-time replays of seeded Poisson arrivals at the
-    offered loads with p50/p99 latency from scheduled arrival to theta on the host."""
+def serving_figures(model, corpus, sweeps: int, rates_arg: str, seconds: float, n_batch: int = 60000) -> dict:
+    """Fold-in serving against a frozen model: one request at a time (max_active=1, closed
+    loop), a saturated batch (all requests queued at once), 32 batched requests again alone
+    (same request ids, so the same randoms), and real-time replays of seeded Poisson
+    arrivals at the offered loads with p50/p99 latency from scheduled arrival to theta on
+    the host.  Requests are new documents from the corpus' generative process, lengths
+    lognormal(median 150, sigma 1.0) in [5, 4000]; theta comes back as FP32[K]."""
     import numpy as np
-    import torch
-    import lda_sc20_b200 as L
-    from lda_sc20_b200.serving import Model, Server
+    from lda_sc20_b200.serving import Server
 
-    torch.cuda.set_device(local)
-    corpus = make_corpus("c1", 0)
-    info = corpus.info
-    K = info.K_hint
-    tr = L.Trainer(corpus, K=K, seed=42, device=local)
-    tr.iterate(100)
-    model = Model(tr)
-    tr.close()
-    sweeps, seed = args.serve_sweeps, 7
+    seed = 7
     rng = np.random.default_rng(11)
     req_seed = [1000]
 
@@ -589,9 +600,6 @@ def run_serving(args, local):
         off, words = corpus.generate_requests(n, req_seed[0])
         return off, words, [words[off[i]:off[i + 1]] for i in range(n)]
 
-    clocks = ClockSampler(physical_gpu(local))
-    clocks.start()
-    # one request at a time
     single = Server(model, sweeps=sweeps, max_active=1, max_tokens=1 << 16, seed=seed)
     _, _, docs1 = requests(300)
     single.run(docs1[:20])
@@ -599,9 +607,8 @@ def run_serving(args, local):
     single.run(docs1)
     single_dps = len(docs1) / (time.perf_counter() - t0)
     single.close()
-    # saturated batch
     batch = Server(model, sweeps=sweeps, max_active=16384, max_tokens=1 << 24, seed=seed)
-    _, _, docsb = requests(60000)
+    _, _, docsb = requests(n_batch)
     batch.run(docsb[:4000])
     s0, l0 = batch.stats()
     t0 = time.perf_counter()
@@ -611,7 +618,6 @@ def run_serving(args, local):
     batch_dps = len(docsb) / batch_s
     tokens_b = int(sum(len(d) for d in docsb))
     batch.close()
-    # 32 of the batch's requests again, one at a time with the same request ids
     alone = Server(model, sweeps=sweeps, max_active=1, max_tokens=1 << 16, seed=seed)
     ident = 0
     for i in range(32):
@@ -621,8 +627,8 @@ def run_serving(args, local):
         ident += int(np.array_equal(r[1].view(np.uint32), th_batch[i].view(np.uint32)))
     alone.close()
     rates = []
-    for rate in [float(x) for x in args.serve_rates.split(",") if x]:
-        n = max(1, int(rate * args.serve_seconds))
+    for rate in [float(x) for x in rates_arg.split(",") if x]:
+        n = max(1, int(rate * seconds))
         off, words, _ = requests(n)
         arrival = np.cumsum(rng.exponential(1.0 / rate, size=n))
         arrival -= arrival[0]
@@ -632,18 +638,72 @@ def run_serving(args, local):
         rates.append({"offered_docs_per_s": rate, "requests": n, "achieved_docs_per_s": n / wall,
                       "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
                       "max_ms": float(lat.max() * 1e3)})
+    return {"docs_per_s": batch_dps, "one_at_a_time_docs_per_s": single_dps,
+            "batch_vs_one_at_a_time": batch_dps / single_dps, "batch_token_sweeps_per_s": tokens_b * sweeps / batch_s,
+            "batch_steps": s1 - s0, "gpu_launches": l1 - l0, "alone_equals_batched": f"{ident}/32",
+            "rates": rates, "sweeps": sweeps}
+
+
+def run_serving(args, local):
+    """Fold-in serving against the word side of the K=1024 corpus trained for 100 sweeps
+    (serving_figures)."""
+    import torch
+    import lda_sc20_b200 as L
+    from lda_sc20_b200.serving import Model
+
+    torch.cuda.set_device(local)
+    corpus = make_corpus("c1", 0)
+    info = corpus.info
+    K = info.K_hint
+    tr = L.Trainer(corpus, K=K, seed=42, device=local)
+    tr.iterate(100)
+    model = Model(tr)
+    tr.close()
+    clocks = ClockSampler(physical_gpu(local))
+    clocks.start()
+    f = serving_figures(model, corpus, args.serve_sweeps, args.serve_rates, args.serve_seconds)
     ck = clocks.stop()
-    line = {"metric": "foldin_docs_per_s", "value": batch_dps, "unit": "docs/s", "n_gpus": 1,
+    model.close()
+    line = {"metric": "foldin_docs_per_s", "value": f["docs_per_s"], "unit": "docs/s", "n_gpus": 1,
             "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"fold-in against the K={K} V={info.vocab} lognormal corpus trained 100 sweeps; "
                                    f"new documents from its generative process, lengths lognormal(median 150, "
-                                   f"sigma 1.0) in [5,4000]; {sweeps} sweeps per request; theta FP32[K]",
-                       "sweeps": sweeps, "K": K, "V": int(info.vocab)},
-            "one_at_a_time_docs_per_s": single_dps, "batch_vs_one_at_a_time": batch_dps / single_dps,
-            "batch_token_sweeps_per_s": tokens_b * sweeps / batch_s,
-            "batch_steps": s1 - s0, "gpu_launches": l1 - l0,
-            "alone_equals_batched": f"{ident}/32", "rates": rates, "clocks": ck}
+                                   f"sigma 1.0) in [5,4000]; {f['sweeps']} sweeps per request; theta FP32[K]",
+                       "sweeps": f["sweeps"], "K": K, "V": int(info.vocab)},
+            **{k: v for k, v in f.items() if k not in ("docs_per_s", "sweeps")}, "clocks": ck}
     print(json.dumps(line), flush=True)
+
+
+def ezlda_leg(sweeps: int = 30) -> dict:
+    """EZLDA's own kernels timed on this B200 (oracle/_ref/ref_harness, built from the
+    reference's sources; a baseline leg, never on the measured path) against this library
+    on the same corpus: the largest shape EZLDA's sparse path takes (K=1024, no dense
+    words, 8 chunks, ~14.5M tokens; its dense-word kernel, which claims segments with an
+    unbounded cross-block spin lock, is never launched)."""
+    import shutil
+    harness = os.path.join(ROOT, "oracle", "_ref", "ref_harness")
+    if not os.path.exists(harness):
+        return {"unavailable": "oracle/_ref/ref_harness is not built (no reference checkout where the build ran)"}
+    from oracle.ref import run_ref
+    tmp = tempfile.mkdtemp(prefix="ezlda_bench_")
+    try:
+        r = run_ref.ezlda_timing(tmp, sweeps)
+    except Exception as e:  # a failed baseline leaves the measured numbers standing
+        return {"unavailable": f"reference harness run failed: {e!r}"[:400]}
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    p = run_ref.REF_TIME
+    return {"corpus": (f"c1 process with D={p['num_docs']} V={p['vocab']} phi~Dir({p['phi_conc']}), K={run_ref.K}, "
+                       f"no dense words, {p['num_chunks']} chunks, seed {p['corpus_seed']}"),
+            "tokens": r["tokens"], "sweeps": r["sweeps"],
+            "ref_ms_per_sweep": r["ref_ms_per_sweep"], "ref_ms_first_last": r["ref_ms_first_last"],
+            "ours_ms": r["ours_ms_per_sweep"], "ours_e2e_ms": r["ours_e2e_ms_per_sweep"],
+            "ratio": r["speedup_resident"], "e2e_ratio": r["speedup_e2e"], "ll_after": r["ll_after"],
+            "host_sweeps_equal_resident": r["host_sweeps_equal_resident"],
+            "timing": ("EZLDA: its own iterStart/iterStop CUDA events per sweep over its two-stream schedule "
+                       "with every chunk copied host<->device (EZLDA/mainKernel.cu:344-347,376); ours: CUDA events "
+                       "around resident sweeps, and wall clock around host-buffer sweeps"),
+            "harness_wall_s": r["harness_wall_s"]}
 
 
 def run_batch(args, local):

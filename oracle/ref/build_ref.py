@@ -3,9 +3,12 @@
 TEST INFRASTRUCTURE ONLY.  Compiles every EZLDA/*.cu of the reference except
 mainKernel.cu (whose main() oracle/ref/ref_harness.cu replaces) for sm_100a, with
 oracle/ref/legacy_shim.h force-included so the pre-Volta warp intrinsics resolve.  The
-sources are read where they lie; nothing is copied into this repository.  Runs only
-where the reference checkout exists (it is absent on GPU machines, which use the
-prebuilt binary)."""
+sources are read where they lie; nothing is copied into this repository.  The EZLDA
+source directory is passed as an argument (or in EZLDA_SRC); with neither, nothing is
+built.  GPU machines have no reference checkout and use the prebuilt binary.
+
+    python oracle/ref/build_ref.py <reference checkout>/EZLDA [--force]
+"""
 from __future__ import annotations
 
 import os
@@ -15,13 +18,13 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE = os.path.dirname(HERE)
 OUT_DIR = os.path.join(ORACLE, "_ref")
-REF_EZLDA = os.environ.get("EZLDA_SRC", "/root/reference/EZLDA")
 REF_SOURCES = ["utility.cu", "DTUpdateKernel.cu", "WTUpdateKernel.cu", "WTDenUpdateKernel.cu", "WTAddKernel.cu",
                "SamplingKernel.cu", "Doc.cu", "DataChunk.cu", "DT.cu", "WT.cu", "WTChunk.cu", "WTDense.cu"]
 
 
-def build(force: bool = False) -> str | None:
-    if not os.path.isdir(REF_EZLDA):
+def build(src: str | None = None, force: bool = False) -> str | None:
+    REF_EZLDA = src or os.environ.get("EZLDA_SRC", "")
+    if not REF_EZLDA or not os.path.isdir(REF_EZLDA):
         return None
     os.makedirs(OUT_DIR, exist_ok=True)
     out = os.path.join(OUT_DIR, "ref_harness")
@@ -44,4 +47,5 @@ def build(force: bool = False) -> str | None:
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv))
+    pos = [a for a in sys.argv[1:] if not a.startswith("--")]
+    print(build(pos[0] if pos else None, force="--force" in sys.argv))

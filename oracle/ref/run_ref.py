@@ -3,14 +3,15 @@ golden fixtures that pin the oracle to the reference.
 
 TEST INFRASTRUCTURE ONLY.  Needs a GPU and the prebuilt oracle/_ref/ref_harness.
 
-    python oracle/ref/run_ref.py OUTDIR [--modes counts,sweeps,dist]
+    python oracle/ref/run_ref.py OUTDIR [--modes=counts,sweeps,dist] [--sweeps=100]
 
 Fixtures written to OUTDIR (then committed under tests/golden/):
   ref_counts.npz   the reference's count rebuild and max-topic outputs on corpus
                    REF_COUNTS (dense and sparse words, K=1024): n_k, sparse WT, dense WT,
                    DT rows, per-token doc metadata, per-word max/2nd/3rd topic, phi and Q
   ref_ll.json      the reference's per-sweep log-likelihood curve (computed with the
-                   oracle's FP64 LL from the reference's topics) on corpus REF_SWEEPS
+                   oracle's FP64 LL from the reference's topics) on corpus REF_SWEEPS,
+                   over 100 sweeps (EZLDA/mainKernel.cu:51 numIters = 100)
   ref_dist.npz     histograms of the reference sampler's draws for tracked tokens over
                    independent sweeps from one state, corpus REF_DIST
 The corpora are regenerated from their generator parameters (stored in each fixture)
@@ -183,7 +184,7 @@ def oracle_ll(o: Oracle, z: np.ndarray) -> float:
     return st.loglik / st.tokens
 
 
-def mode_sweeps(tmp, out, n=30):
+def mode_sweeps(tmp, out, n=100):
     c = make_corpus(REF_SWEEPS)
     i = c.info
     d = os.path.join(tmp, "sweeps")
@@ -236,20 +237,24 @@ def mode_dist(tmp, out, reps=2000, stride=25):
             "frac_p_below_0.01": float((pvals < 0.01).mean())}
 
 
-def mode_time(tmp, out, n=30):
+def ezlda_timing(tmp, n=30, corpus=None):
     """EZLDA's per-sweep time (its own iterStart/iterStop events over its two-stream
-    schedule, host<->device chunk copies included) against this library on the same
-    corpus and sweeps: resident (lda_trainer_iterate) and through host buffers
-    (lda_iterate_host_async, topics uploaded and downloaded chunk by chunk every sweep)."""
+    schedule, host<->device chunk copies included; EZLDA/mainKernel.cu:344-347,376) against
+    this library on the same corpus and sweeps: resident (lda_trainer_iterate, CUDA events)
+    and through host buffers (lda_iterate_host_async, topics uploaded and downloaded chunk
+    by chunk every sweep, wall clock).  Both start from the corpus' initial topics; the LL
+    of both final states is scored by the oracle's FP64 formula."""
     import time as _time
     import torch
-    c = make_corpus(REF_TIME)
+    c = corpus if corpus is not None else make_corpus(REF_TIME)
     i = c.info
     d = os.path.join(tmp, "time")
     c.write_ezlda(d, K)
     dump = os.path.join(tmp, "time_out")
     os.makedirs(dump)
+    t_ref = _time.perf_counter()
     log = run_harness("time", d, dump, n)
+    t_ref = _time.perf_counter() - t_ref
     ref_ms = np.fromfile(os.path.join(dump, "sweep_ms.f32"), dtype=np.float32)
     z_ref = np.fromfile(os.path.join(dump, "topics_last.u16"), dtype=np.uint16) - 1
     tr = L.Trainer(c, K=K, alpha=float(ALPHA), beta=float(BETA), seed=42)
@@ -269,20 +274,30 @@ def mode_time(tmp, out, n=30):
     z_ours = tr.topics()
     a = torch.from_numpy(z0.view(np.int16).copy()).pin_memory()
     b = torch.empty_like(a).pin_memory()
+    tr.set_topics(z0)
     tr.iteration = 0
+    torch.cuda.synchronize()
     t0 = _time.perf_counter()
     for _ in range(n):
         tr.iterate_host_async(a.numpy().view(np.uint16), b.numpy().view(np.uint16))
         a, b = b, a
     tr.wait()
     e2e_ms = 1e3 * (_time.perf_counter() - t0) / n
+    same = bool(np.array_equal(a.numpy().view(np.uint16), z_ours))
+    tr.close()
     o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, ALPHA, BETA)
     ll_ref, ll_ours = oracle_ll(o, z_ref.astype(np.uint16)), oracle_ll(o, z_ours)
-    res = {"log": log.strip(), "tokens": i.num_tokens, "sweeps": n,
-           "ref_ms_per_sweep": float(ref_ms.mean()), "ref_ms_first_last": [float(ref_ms[0]), float(ref_ms[-1])],
-           "ours_ms_per_sweep": ours_ms, "ours_e2e_ms_per_sweep": e2e_ms,
-           "speedup_resident": float(ref_ms.mean()) / ours_ms, "speedup_e2e": float(ref_ms.mean()) / e2e_ms,
-           "ll_after": {"ref": ll_ref, "ours": ll_ours}}
+    o.close()
+    return {"log": log.strip(), "tokens": i.num_tokens, "sweeps": n, "harness_wall_s": t_ref,
+            "ref_ms_per_sweep": float(ref_ms.mean()), "ref_ms_first_last": [float(ref_ms[0]), float(ref_ms[-1])],
+            "ours_ms_per_sweep": ours_ms, "ours_e2e_ms_per_sweep": e2e_ms,
+            "speedup_resident": float(ref_ms.mean()) / ours_ms, "speedup_e2e": float(ref_ms.mean()) / e2e_ms,
+            "host_sweeps_equal_resident": same,
+            "ll_after": {"ref": ll_ref, "ours": ll_ours, "rel_diff": abs(ll_ours - ll_ref) / abs(ll_ref)}}
+
+
+def mode_time(tmp, out, n=30):
+    res = ezlda_timing(tmp, n)
     with open(os.path.join(out, "ref_time.json"), "w") as f:
         json.dump({"params": REF_TIME, **res}, f, indent=1)
     return res
@@ -304,15 +319,19 @@ def _chi2_pvalue(h, p, n, chi2):
 def main():
     out = sys.argv[1] if len(sys.argv) > 1 else "ref_out"
     modes = "counts,sweeps,dist"
+    sweeps = 100
     for a in sys.argv[2:]:
         if a.startswith("--modes="):
             modes = a.split("=", 1)[1]
+        elif a.startswith("--sweeps="):
+            sweeps = int(a.split("=", 1)[1])
     os.makedirs(out, exist_ok=True)
     tmp = tempfile.mkdtemp(prefix="ezlda_ref_")
     summary = {}
     try:
         for m in modes.split(","):
-            fn = {"counts": mode_counts, "sweeps": mode_sweeps, "dist": mode_dist, "time": mode_time}[m]
+            fn = {"counts": mode_counts, "sweeps": lambda t, o: mode_sweeps(t, o, sweeps), "dist": mode_dist,
+                  "time": mode_time}[m]
             try:
                 summary[m] = fn(tmp, out)
             except Exception as e:  # record and continue with the other modes

@@ -111,6 +111,41 @@ def test_k_variants(K):
     del tr
 
 
+@pytest.mark.parametrize("K,preset,alpha,stream_mode", [
+    (4096, "c0", None, 1), (4096, "c0", None, 2), (10000, "c1", 0.1, 1), (10000, "c1", 0.1, 2)])
+def test_large_k_dense_words_bit_exact(K, preset, alpha, stream_mode):
+    """Above 2048 topics dense words go to the CTA-per-tile dense-word sampler and sparse
+    words to the column-free one (the path of LDAKernelTrainD + UpdateProbKernelTrainD1,
+    EZLDA/utility.cu:1625-2103, :2680-3312, and LDAKernelTrain, :1217-1611).  Corpora with
+    dense words, resident and streamed, plain and LL sweeps: topics equal the oracle's token
+    for token after every sweep and the FP64 LL is within 1e-9.  The K=10,000 case uses
+    Zipfian word frequencies, so frequent dense words span several 2048-token tiles."""
+    if preset == "c0":
+        cfg = L.corpus_config("c0", num_docs=2000, vocab=5000, K=K, num_chunks=3, dense_kind=1, dense_param=0.05)
+    else:
+        cfg = L.corpus_config("c1", num_docs=3000, vocab=6000, K=K, num_chunks=3, corpus_seed=99)
+    c = L.Corpus.generate(cfg)
+    i = c.info
+    assert i.num_dense > 0
+    tr = L.Trainer(c, K=K, alpha=alpha, seed=11, stream_mode=stream_mode, num_streams=2)
+    assert tr.stream_info()[0] is (stream_mode == 2)
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta)
+    z = c.topics()
+    for it in range(3):
+        ll = it != 1  # sweeps 0 and 2 run the LL-mode kernels, sweep 1 the plain ones
+        st = o.iterate(z, 11, it, ll=ll)
+        tr.reset_stats()
+        tr.iterate(1, ll=ll)
+        if ll:
+            s, _ = tr.loglik()
+            assert abs(s - st.loglik) <= LL_RTOL * abs(st.loglik), f"LL at sweep {it}"
+        zg = tr.topics()
+        assert np.array_equal(zg, z), f"sweep {it}: {(zg != z).sum()} of {len(z)} topics differ"
+        cnt = tr.counters()
+        assert cnt.word_tiles_dense > 0 and cnt.word_tiles_sparse > 0
+        assert (cnt.branch_max, cnt.branch_s, cnt.branch_q) == (st.branch_max, st.branch_s, st.branch_q)
+
+
 def test_mid_size_k1024_lognormal():
     cfg = L.corpus_config("c1", num_docs=20000, vocab=20000, num_chunks=4, corpus_seed=77)
     c = L.Corpus.generate(cfg)
