@@ -5,8 +5,8 @@ iteration-start counts, a chunk's draws depend only on the global word-topic cou
 sweep's starting topics.  Each rank keeps the whole corpus layout resident, rebuilds the
 word-topic counts from the full topic array (replicated, ~0.8 ms for 72M tokens), and runs
 the doc-topic rebuild and the sampler for its own contiguous range of chunks.  After every
-sweep each rank broadcasts its chunks' topic slice in place (uint16, 2 bytes per token),
-which is the only exchange.  Randoms are keyed on the global token index, so the result is
+sweep one all-gather moves each rank's chunks' topic slice (uint16, 2 bytes per token) to
+every rank, which is the only exchange.  Randoms are keyed on the global token index, so the result is
 bit-identical to one GPU with the same chunking.
 """
 from __future__ import annotations
@@ -22,21 +22,34 @@ def shard_chunks(num_chunks: int, world: int) -> list[tuple[int, int]]:
 
 
 class TopicExchange:
-    """Broadcasts each rank's topic slice [chunk_tok[first], chunk_tok[last]) to all ranks,
-    in place in a 1-D 16-bit tensor (CUDA with NCCL, CPU with gloo).  Neither backend has
-    a 16-bit integer type, so the slices travel as bytes."""
+    """After a sweep each rank holds new topics only for its own chunks' tokens, one
+    contiguous slice [chunk_tok[first], chunk_tok[last]) of the word-sorted 16-bit topic
+    array.  One all-gather moves every slice to every rank: each rank's slice is copied
+    into an equal-sized send segment (padded to the longest slice), the segments are
+    gathered into one buffer, and the other ranks' slices are copied into place.  Neither
+    NCCL nor gloo has a 16-bit integer type, so the slices travel as bytes.  Works on CUDA
+    tensors with NCCL and on CPU tensors with gloo."""
 
     def __init__(self, topics, chunk_tok, ranges, group=None):
         import torch
+        import torch.distributed as dist
         self.t = topics.view(torch.uint8)
         self.slices = [(2 * int(chunk_tok[a]), 2 * int(chunk_tok[b])) for a, b in ranges]
         self.group = group
+        self.rank = dist.get_rank(group) if dist.is_initialized() else 0
+        self.seg = max(1, max(b - a for a, b in self.slices))
+        self.seg = (self.seg + 15) & ~15  # 16-byte segments
+        self.send = torch.zeros(self.seg, dtype=torch.uint8, device=topics.device)
+        self.recv = torch.empty(len(ranges) * self.seg, dtype=torch.uint8, device=topics.device)
 
     def exchange(self) -> None:
         import torch.distributed as dist
-        for src, (a, b) in enumerate(self.slices):
-            if b > a:
-                dist.broadcast(self.t[a:b], src=src, group=self.group)
+        a, b = self.slices[self.rank]
+        self.send[:b - a].copy_(self.t[a:b])
+        dist.all_gather_into_tensor(self.recv, self.send, group=self.group)
+        for r, (a, b) in enumerate(self.slices):
+            if r != self.rank and b > a:
+                self.t[a:b].copy_(self.recv[r * self.seg:r * self.seg + (b - a)])
 
 
 class _CudaArray:

@@ -1,5 +1,6 @@
-"""Document-sharded sweeps: the exchange logic on CPU with gloo (world size 2), and the
-sharded algorithm on one GPU with two trainers standing in for two ranks."""
+"""Document-sharded sweeps: the exchange on CPU with gloo (world size 2), real sharded
+sweeps of the oracle through that exchange on two CPU ranks, and the sharded algorithm on
+one GPU with two trainers standing in for two ranks."""
 import os
 import socket
 
@@ -58,6 +59,59 @@ def test_topic_exchange_gloo_world2():
         expect[s:e] = (np.arange(s, e) % 1000 + 7 * r).astype(np.int16)
     for r in range(world):
         assert np.array_equal(res[r], expect)
+
+
+def _sharded_worker(rank, world, port, params, sweeps, out):
+    """One rank of a document-sharded sweep on CPU: the oracle rebuilds the counts from the
+    full topic array, samples only this rank's chunks' documents, and the real TopicExchange
+    (gloo all-gather) brings in the other ranks' slices."""
+    import torch.distributed as dist
+    from oracle import Oracle
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
+    p = dict(params)
+    c = L.Corpus.generate(L.corpus_config(p.pop("preset"), **p))
+    i = c.info
+    ranges = shard_chunks(i.num_chunks, world)
+    cd = c.chunk_doc()
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, 64, 50.0 / 64, 0.01, nthreads=2)
+    o.set_doc_range(int(cd[ranges[rank][0]]), int(cd[ranges[rank][1]]))
+    z = torch.from_numpy(c.topics().view(np.int16).copy())
+    ex = TopicExchange(z, c.chunk_tok(), ranges)
+    lls = []
+    for it in range(sweeps):
+        zz = z.numpy().view(np.uint16)
+        st = o.iterate(zz, 42, it, ll=True)
+        v = torch.tensor([st.loglik, float(st.tokens)], dtype=torch.float64)
+        dist.all_reduce(v)
+        lls.append(float(v[0]))
+        ex.exchange()
+    out[rank] = (z.numpy().view(np.uint16).copy(), lls)
+    dist.destroy_process_group()
+
+
+def test_sharded_oracle_sweeps_gloo_world2():
+    """Two CPU ranks run real document-sharded sweeps (each samples its half of the chunks,
+    then the gloo all-gather exchange) for four sweeps: every rank ends with the topics of
+    one process sweeping all chunks, and the summed LL partials equal its LL."""
+    from oracle import Oracle
+    params = dict(preset="c0", num_docs=600, vocab=1500, num_chunks=4, dense_kind=1, dense_param=0.05)
+    sweeps, world = 4, 2
+    port = _free_port()
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_sharded_worker, args=(world, port, params, sweeps, out), nprocs=world, join=True)
+        res = [out[r] for r in range(world)]
+    p = dict(params)
+    c = L.Corpus.generate(L.corpus_config(p.pop("preset"), **p))
+    i = c.info
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, 64, 50.0 / 64, 0.01, nthreads=2)
+    z = c.topics()
+    for it in range(sweeps):
+        st = o.iterate(z, 42, it, ll=True)
+        for r in range(world):
+            assert abs(res[r][1][it] - st.loglik) <= 1e-9 * abs(st.loglik), (r, it)
+    for r in range(world):
+        assert np.array_equal(res[r][0], z), f"rank {r}: {(res[r][0] != z).sum()} topics differ"
 
 
 @pytest.mark.gpu
