@@ -294,7 +294,21 @@ typedef struct {
     const uint32_t* dt_nnz;        /* [D] */
     const uint32_t* dt_ent;
     double* ll_sum;                /* device scalar, written when ll_mode */
+    /* lengths of the caller's buffers, for the range checks below */
+    int64_t num_tokens;            /* entries of tok_doc, meta and topics */
+    int32_t num_docs;              /* entries of doc_len, dt_off and dt_nnz */
+    int64_t num_dt_entries;        /* entries of dt_ent */
+    int64_t num_sparse_entries;    /* entries of sparse_ent */
+    int32_t* status;               /* device int32, written every call (LDA_IO_* bits; 0 = sampled) */
 } lda_sample_io;
+
+/* Bits of *io->status: a check that failed on the device.  When any is set no token is
+ * sampled (topics are left as they were) and ll_sum is not meaningful. */
+#define LDA_IO_TILE 1        /* a tile's word is outside [0, vocab) or its tokens outside [0, num_tokens) */
+#define LDA_IO_MAX_TOPIC 2   /* a tile word's max topic (top2 & 0xffff) is >= K */
+#define LDA_IO_WORD_ROW 4    /* a sparse word's row leaves sparse_ent or holds a topic >= K */
+#define LDA_IO_TOKEN_DOC 8   /* a tile token's doc id is >= num_docs */
+#define LDA_IO_DOC_ROW 16    /* a doc row leaves dt_ent or holds a topic >= K */
 
 /* Samples the tokens of io->tiles exactly as lda_sample_chunk does, but allocates
  * nothing: no cudaMalloc, cudaFree or allocating library call.  It exists for callers
@@ -306,12 +320,23 @@ typedef struct {
  *
  * Its scratch (tile counter, sweep counters, per-tile LL partials) is one file-scope
  * device array of 524,544 bytes that every GPU loading the library holds until the
- * process exits.  Limits: num_tiles <= 65536 (LDA_ERR_ARG beyond), K <= the largest K a
- * trainer accepts.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress with that device current); make that first call before any
- * stream capture.  Every call shares the array, so calls that overlap on the GPU (on
- * different streams or devices sharing a context) race; serialise them.  The call is
- * asynchronous on `stream` (NULL: the legacy default stream) and sets `device` current. */
+ * process exits.  Limits: num_tiles <= 65536 (LDA_ERR_ARG beyond); K at most what one
+ * warp's word column plus the CTA's reciprocal table fit in shared memory, about 28,000
+ * topics on a B200 (LDA_ERR_ARG beyond).  Every K runs the per-warp-column sampler the
+ * trainer uses up to 2048 topics; above that the trainer splits dense and sparse words
+ * over two other kernels, and this entry point draws the same topics with one.
+ *
+ * The caller's indices are checked on the device before any token is sampled: a kernel
+ * checks every tile, the max topic and sparse row of every tile's word, every tile
+ * token's doc id and every doc row against K and the buffer lengths above, and writes the
+ * failed checks to *io->status (0 when all pass; read it after the stream's work).  A
+ * failure stops the sampling kernel from taking any tile, so bad input never indexes
+ * memory.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress with that device current) and keeps it for the process; make that
+ * first call before any stream capture, and do not reset the device (cudaDeviceReset)
+ * after it.  Every call shares the array, so calls that overlap on the GPU (on different
+ * streams or devices sharing a context) race; serialise them.  The call is asynchronous on
+ * `stream` (NULL: the legacy default stream) and sets `device` current. */
 int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream);
 
 /* ------------------------------------------------ batched training */

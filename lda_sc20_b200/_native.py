@@ -77,6 +77,8 @@ class SampleIO(C.Structure):
         ("ql", C.c_void_p), ("tok_doc", C.c_void_p), ("meta", C.c_void_p), ("topics", C.c_void_p),
         ("doc_len", C.c_void_p), ("dt_off", C.c_void_p), ("dt_nnz", C.c_void_p), ("dt_ent", C.c_void_p),
         ("ll_sum", C.c_void_p),
+        ("num_tokens", C.c_int64), ("num_docs", C.c_int32), ("num_dt_entries", C.c_int64),
+        ("num_sparse_entries", C.c_int64), ("status", C.c_void_p),
     ]
 
 

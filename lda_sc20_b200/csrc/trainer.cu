@@ -1402,6 +1402,75 @@ unsigned char* g_noalloc_addr[kMaxDevices] = {};
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
 
+namespace {
+// What k_check_sample_io reads: the indices of an allocation-free call that the sampler
+// would follow, with the lengths of the buffers they index.
+struct IoCheck {
+    const int4* tiles;
+    int ntiles, K, V, Vd, D;
+    const uint32_t* top2;
+    const uint32_t* swt_off;
+    const uint32_t* swt_nnz;
+    const uint32_t* swt_ent;
+    const uint32_t* tok_doc;
+    const uint32_t* dt_off;
+    const uint32_t* dt_nnz;
+    const uint32_t* dt_ent;
+    int64_t N, n_dt, n_sp;
+    int* status;
+    unsigned* tile_counter;
+};
+}  // namespace
+
+// Range checks before an allocation-free sampling launch: warp per tile (its word, token
+// range, the word's max topic and sparse row, its tokens' doc ids), thread per doc (its
+// row's extent and topics).  A failure ORs LDA_IO_* bits into *status and moves the tile
+// counter past any tile index, so the sampling kernel that follows on the stream takes no
+// tile (its warps' first claim returns >= ntiles; the counter stays below 2^31).
+__global__ void __launch_bounds__(256) k_check_sample_io(IoCheck c) {
+    const int lane = threadIdx.x & 31;
+    const int gw = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5), nw = (int)((gridDim.x * blockDim.x) >> 5);
+    int bad = 0;
+    for (int t = gw; t < c.ntiles; t += nw) {
+        const int4 tl = c.tiles[t];
+        if (tl.x < 0 || tl.x >= c.V || tl.y < 0 || tl.z < 0 || (int64_t)tl.y + tl.z > c.N) {
+            bad |= LDA_IO_TILE;
+            continue;
+        }
+        const int w = tl.x;
+        if ((c.top2[w] & 0xffffu) >= (uint32_t)c.K) bad |= LDA_IO_MAX_TOPIC;
+        if (w >= c.Vd) {
+            const int sw = w - c.Vd;
+            const uint64_t off = c.swt_off[sw], nnz = c.swt_nnz[sw];
+            if (off + nnz > (uint64_t)c.n_sp) {
+                bad |= LDA_IO_WORD_ROW;
+            } else {
+                for (uint64_t e = (uint64_t)lane; e < nnz; e += 32u)
+                    if ((c.swt_ent[off + e] >> 16) >= (uint32_t)c.K) bad |= LDA_IO_WORD_ROW;
+            }
+        }
+        for (int i = lane; i < tl.z; i += 32)
+            if (c.tok_doc[(int64_t)tl.y + i] >= (uint32_t)c.D) bad |= LDA_IO_TOKEN_DOC;
+    }
+    for (int d = (int)(blockIdx.x * blockDim.x + threadIdx.x); d < c.D; d += (int)(gridDim.x * blockDim.x)) {
+        const uint64_t off = c.dt_off[d], nnz = c.dt_nnz[d];
+        if (off + nnz > (uint64_t)c.n_dt) {
+            bad |= LDA_IO_DOC_ROW;
+            continue;
+        }
+        for (uint64_t e = 0; e < nnz; ++e) {
+            if ((c.dt_ent[off + e] >> 16) >= (uint32_t)c.K) {
+                bad |= LDA_IO_DOC_ROW;
+                break;
+            }
+        }
+    }
+    if (bad) {
+        atomicOr(c.status, bad);
+        atomicExch(c.tile_counter, 1u << 30);
+    }
+}
+
 static int noalloc_scratch(int device, unsigned char** out) {
     if (device < 0 || device >= kMaxDevices) return fail(LDA_ERR_ARG, "device %d out of range", device);
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
@@ -1431,6 +1500,9 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
         return fail(LDA_ERR_ARG, "null device buffer in lda_sample_io");
     if (((uintptr_t)io->tiles & 15u) || ((uintptr_t)io->dt_ent & 15u) || ((uintptr_t)io->phi4 & 15u))
         return fail(LDA_ERR_ARG, "tiles, phi4 and dt_ent must be 16-byte aligned");
+    if (!io->status) return fail(LDA_ERR_ARG, "null status word in lda_sample_io");
+    if (io->num_tokens < 0 || io->num_docs < 0 || io->num_dt_entries < 0 || io->num_sparse_entries < 0)
+        return fail(LDA_ERR_ARG, "negative buffer length in lda_sample_io");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
         cudaGetLastError();
@@ -1442,6 +1514,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     if (rc) return rc;
     cudaStream_t st = (cudaStream_t)stream_ptr;
     CUDA_TRY(cudaMemsetAsync(scratch, 0, kNoAllocHeader, st));  // tile counter + sweep counters
+    CUDA_TRY(cudaMemsetAsync(io->status, 0, sizeof(int32_t), st));
     if (io->num_tiles == 0) {
         if (io->ll_mode) CUDA_TRY(cudaMemsetAsync(io->ll_sum, 0, sizeof(double), st));
         return LDA_OK;
@@ -1476,6 +1549,14 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
     a.tok_base = 0;
     a.dt_base = 0;
+    IoCheck chk;
+    chk.tiles = a.tiles; chk.ntiles = io->num_tiles; chk.K = io->K; chk.V = io->vocab; chk.Vd = io->num_dense;
+    chk.D = io->num_docs; chk.top2 = io->top2; chk.swt_off = io->sparse_off; chk.swt_nnz = io->sparse_nnz;
+    chk.swt_ent = io->sparse_ent; chk.tok_doc = io->tok_doc; chk.dt_off = io->dt_off; chk.dt_nnz = io->dt_nnz;
+    chk.dt_ent = io->dt_ent; chk.N = io->num_tokens; chk.n_dt = io->num_dt_entries;
+    chk.n_sp = io->num_sparse_entries; chk.status = io->status; chk.tile_counter = a.tile_counter;
+    k_check_sample_io<<<4 * num_sms, 256, 0, st>>>(chk);
+    CUDA_TRY(cudaGetLastError());
     launch_sample(a.ll_mode != 0, io->K, grid, 32 * warps, smem, st, a);
     CUDA_TRY(cudaGetLastError());
     if (io->ll_mode) {
