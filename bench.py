@@ -102,16 +102,22 @@ def measured_peaks():
         return {"hbm_gbs": HBM_FALLBACK_GBS}, "fallback"
 
 
-def ncu_traffic(preset: str, chunks: int = 0):
-    """Per-launch DRAM bytes of the sampler from the committed ncu summary of this workload
-    (profiles/k_sample_<preset>_traffic.json), if there is one for its default chunking."""
-    if chunks:
+def ncu_traffic(preset: str, tokens_per_launch: float):
+    """Per-launch DRAM bytes (read + write) of the sampler: the bytes per token of a small
+    ncu capture of the same kernel on the one-fifth K=1024 corpus
+    (profiles/k_sample_c1s_traffic.json, a few launches), scaled by this run's tokens per
+    launch.  The sampler's DRAM traffic is per-token data (token docs, metadata, topics)
+    plus word columns; doc rows come from L2, so it grows with the tokens."""
+    if preset not in ("c1", "c1s"):
         return None
-    path = os.path.join(ROOT, "profiles", f"k_sample_{preset}_traffic.json")
+    path = os.path.join(ROOT, "profiles", "k_sample_c1s_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f)
-    except (OSError, ValueError):
+            t = json.load(f)
+        return {"dram_bytes_per_launch": float(t["dram_bytes_per_token"]) * tokens_per_launch,
+                "source": f"profiles/k_sample_c1s_traffic.json ({t['dram_bytes_per_token']:.1f} B/token) "
+                          f"x {tokens_per_launch:.0f} tokens per launch"}
+    except (OSError, ValueError, KeyError):
         return None
 
 
@@ -414,7 +420,7 @@ def run_ours(args, world, rank, local):
         achieved = None  # the timed stage spans the chunk copies, doc-row rebuilds and sampling
     peaks, peak_src = measured_peaks()
     peak = float(peaks.get("hbm_gbs", HBM_FALLBACK_GBS))
-    traffic = ncu_traffic(args.preset, args.chunks)
+    traffic = ncu_traffic(args.preset, cnt.tokens / max(launches_sample, 1))
 
     # end to end through the C ABI with pinned host buffers: upload topics, sweep, download
     e2e = None
@@ -484,6 +490,7 @@ def run_ours(args, world, rank, local):
             "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic.get("dram_bytes_per_launch") if traffic else None,
+                         "traffic_source": traffic.get("source") if traffic else None,
                          "peak_source": f"{peak_src} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg_bytes / max(launches_sample, 1),
                          "ms_per_launch": ms_per_launch},

@@ -318,13 +318,15 @@ typedef struct {
  * device, fragment the pool, or fail with out-of-memory in the middle of a request.
  * No counterpart in the reference: EZLDA allocates everything up front in its classes.
  *
- * Its scratch (tile counter, sweep counters, per-tile LL partials) is one file-scope
- * device array of 524,544 bytes that every GPU loading the library holds until the
- * process exits.  Limits: num_tiles <= 65536 (LDA_ERR_ARG beyond); K at most what one
- * warp's word column plus the CTA's reciprocal table fit in shared memory, about 28,000
- * topics on a B200 (LDA_ERR_ARG beyond).  Every K runs the per-warp-column sampler the
- * trainer uses up to 2048 topics; above that the trainer splits dense and sparse words
- * over two other kernels, and this entry point draws the same topics with one.
+ * Its scratch (tile counter, sweep counters, per-tile LL partials and, above 2048 topics,
+ * the smoothing table of the sparse words' split Q bucket) is one file-scope device array
+ * of 643,328 bytes that every GPU loading the library holds until the process exits.
+ * Limits: num_tiles <= 65536 (LDA_ERR_ARG beyond); K at most what one warp's word column
+ * plus the CTA's reciprocal table fit in shared memory, about 28,000 topics on a B200
+ * (LDA_ERR_ARG beyond).  Every K runs the per-warp-column sampler the trainer uses up to
+ * 2048 topics; above that the trainer splits dense and sparse words over two other
+ * kernels, and this entry point draws the same topics with one.  Doc-row keys are topics
+ * (the layout lda_get_doc_rows returns).
  *
  * The caller's indices are checked on the device before any token is sampled: a kernel
  * checks every tile, the max topic and sparse row of every tile's word, every tile

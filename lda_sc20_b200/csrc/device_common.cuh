@@ -13,6 +13,12 @@ namespace dev {
 
 constexpr unsigned FULL = 0xffffffffu;
 
+// Above this many topics the trainer samples with the CTA-per-tile dense-word kernel and
+// the column-free sparse-word kernel (kernels.cuh) instead of a column per warp, and a
+// sparse word's Q bucket is split into its own topics and a word-independent smoothing
+// part (split_q_draw).
+constexpr int kLargeK = 2048;
+
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
@@ -249,6 +255,26 @@ __device__ __forceinline__ int warp_level2_rounds(uint32_t n, float t2, int fall
     return last >= 0 ? last : fallback;
 }
 
+// First k in [lo, hi) with x < T[k] for a non-decreasing table T in global memory, else
+// -1; uniform across the warp.  A 32-way search: each round the lanes probe the ends of 32
+// equal segments of the range, and a ballot keeps the first segment whose end exceeds x
+// (the answer lies in it, since every entry before its start is <= x).
+__device__ __forceinline__ int warp_first_above(const float* __restrict__ T, int lo, int hi, float x, int lane) {
+    if (lo >= hi || !(x < __ldg(T + hi - 1))) return -1;
+    while (hi - lo > 32) {
+        const int step = (hi - lo + 31) >> 5;
+        const int p = min(lo + (lane + 1) * step - 1, hi - 1);
+        const unsigned b = __ballot_sync(FULL, x < __ldg(T + p));  // lane 31 probes hi - 1
+        const int f = __ffs(b) - 1;
+        const int nlo = f == 0 ? lo : min(lo + f * step - 1, hi - 1) + 1;
+        hi = min(lo + (f + 1) * step - 1, hi - 1) + 1;
+        lo = nlo;
+    }
+    const int p = lo + lane;
+    const unsigned b = __ballot_sync(FULL, p < hi && x < __ldg(T + p));
+    return lo + __ffs(b) - 1;
+}
+
 // Rounds of the Q-bucket search of one lane slot ls whose (round total, largest lane
 // prefix) pairs the dense-word sampler keeps per tile: R = ceil(ceil(K/32) / 32) rounds of
 // 32 slots, for 2 <= R <= 16 (above that the table is not kept).
@@ -284,31 +310,56 @@ __device__ __forceinline__ int warp_level2_table(uint32_t n, float t2, int lane,
     return -1;
 }
 
+// Doc-row entries are (key << 16) | count.  Up to kLargeK topics the trainer's rows carry
+// the word column's slot index col_skew(k) as the key, so a lookup needs no index
+// arithmetic; above kLargeK, and in rows a caller supplies, the key is the topic k.
+// col_skew is k + k/32, so k = s - s/33 inverts it (s = 33a + b with b < 32).
+__host__ __device__ __forceinline__ int col_unskew(int s) { return s - s / 33; }
+
 // The sampler's view of the tile's word column: colz(k) = phi_k of the word with its max
-// topic zeroed.  ColShared reads a column built in shared memory (skewed layout, with the
-// max topic's slot already zeroed).
-struct ColShared {
+// topic zeroed; row(key) the same for a doc-row key and topic(key) the key's topic.
+// ColSharedT reads a column built in shared memory (skewed layout, with the max topic's
+// slot already zeroed); SKEWKEYS: the rows' keys are slot indices.
+template <bool SKEWKEYS>
+struct ColSharedT {
     const float* col;
     __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
+    __device__ __forceinline__ float row(uint32_t key) const { return col[SKEWKEYS ? (int)key : col_skew((int)key)]; }
+    __device__ __forceinline__ int topic(uint32_t key) const { return SKEWKEYS ? col_unskew((int)key) : (int)key; }
 };
+using ColShared = ColSharedT<false>;
 
 // Serial per-lane sum over the lane's entries l, l + 32, l + 64, ... of a doc row of nnz
 // entries (one fmaf chain).  A warp's loads of one step then read 32 consecutive entries,
 // one or two 128-byte lines, where contiguous per-lane blocks would touch one line per
-// lane block.  The loads of two steps are issued together.
+// lane block.
+#ifndef LDA_ROW_MODE
+#define LDA_ROW_MODE 0
+#endif
 template <class View>
 __device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uint32_t lane, uint32_t nnz,
-                                           const View& colz) {
-    float acc = 0.0f;
+                                           const View& colz, float acc = 0.0f) {
     uint32_t q = lane;
+#if LDA_ROW_MODE == 1
+    // the loads of four steps, then of two, then one, issued before their use
+    for (; q + 96u < nnz; q += 128u) {
+        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
+                       e3 = __ldg(row + q + 96u);
+        acc = ffma(u2f(e0 & 0xffffu), colz.row(e0 >> 16), acc);
+        acc = ffma(u2f(e1 & 0xffffu), colz.row(e1 >> 16), acc);
+        acc = ffma(u2f(e2 & 0xffffu), colz.row(e2 >> 16), acc);
+        acc = ffma(u2f(e3 & 0xffffu), colz.row(e3 >> 16), acc);
+    }
+#endif
+    // the loads of two steps issued together
     for (; q + 32u < nnz; q += 64u) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
-        acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
-        acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
+        acc = ffma(u2f(e0 & 0xffffu), colz.row(e0 >> 16), acc);
+        acc = ffma(u2f(e1 & 0xffffu), colz.row(e1 >> 16), acc);
     }
     if (q < nnz) {
         const uint32_t e = __ldg(row + q);
-        acc = ffma(u2f(e & 0xffffu), colz((int)(e >> 16)), acc);
+        acc = ffma(u2f(e & 0xffffu), colz.row(e >> 16), acc);
     }
     return acc;
 }
@@ -330,16 +381,16 @@ __device__ __forceinline__ int lane_draw(const uint32_t* __restrict__ row, uint3
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             if (q + 32u * s >= nnz) break;
-            const int k = (int)(e[s] >> 16);
-            const float cz = colz(k);
+            const uint32_t key = e[s] >> 16;
+            const float cz = colz.row(key);
             acc = ffma(u2f(e[s] & 0xffffu), cz, acc);
             if (cz > 0.0f) {
-                last = k;
-                if (t2 < acc) return k;
+                last = (int)key;
+                if (t2 < acc) return colz.topic(key);
             }
         }
     }
-    return last >= 0 ? last : fallback;
+    return last >= 0 ? colz.topic((uint32_t)last) : fallback;
 }
 
 

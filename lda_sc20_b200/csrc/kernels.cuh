@@ -73,8 +73,9 @@ __global__ void __launch_bounds__(256) k_dt_build(DtArgs a) {
     }
 }
 
-// Sampler: warp per tile, tiles taken from an atomic counter.
-template <bool LL, int QB = 1>
+// Sampler: warp per tile, tiles taken from an atomic counter.  SKEWKEYS: the doc rows'
+// keys are word-column slot indices (the trainer's rows up to kLargeK topics).
+template <bool LL, int QB = 1, bool SKEWKEYS = true>
 __global__ void __launch_bounds__(32 * kSampleWarps, LL ? LDA_SAMPLE_LL_MIN_BLOCKS
                                                        : (QB == 1 ? LDA_SAMPLE_MIN_BLOCKS : LDA_SAMPLE_QB_MIN_BLOCKS))
 k_sample_t(SampleArgs a) {
@@ -92,7 +93,7 @@ k_sample_t(SampleArgs a) {
         tile = __shfl_sync(FULL, tile, 0);
         if (tile >= a.ntiles) break;
         const int4 t = a.tiles[tile];
-        sample_tile<LL, QB>(a, tile, t, a.iter, r, col, ctr, lane);
+        sample_tile<LL, QB, SKEWKEYS>(a, tile, t, a.iter, r, col, ctr, lane);
     }
     __syncwarp();
     if (lane < C_NUM && ctr[lane]) atomicAdd(a.ctr + lane, (unsigned long long)ctr[lane]);
@@ -126,6 +127,8 @@ struct ColBits {
         }
         return fmul(beta, rk);
     }
+    __device__ __forceinline__ float row(uint32_t key) const { return (*this)((int)key); }
+    __device__ __forceinline__ int topic(uint32_t key) const { return (int)key; }
 };
 
 __host__ __device__ __forceinline__ int large_bit_words(int K) { return (K + 31) >> 5; }
@@ -213,8 +216,9 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         const float Q = __shfl_sync(FULL, QP, 31);
         __syncwarp();
         const ColBits view{bits, pre, ent, r, a.beta, maxK};
-        double ll = sample_groups<LL, QB>(a, (uint32_t)t.y, (uint32_t)t.z, 0u, 32u, a.iter, maxK, ph, QL, QP, Q, view,
-                                          ctr, lane);
+        const SplitQ sq{ent, nnz_w, __shfl_sync(FULL, QL, 0), a.smooth, r, true};
+        double ll = sample_groups<LL, QB, true>(a, (uint32_t)t.y, (uint32_t)t.z, 0u, 32u, a.iter, maxK, ph, QL, QP, Q,
+                                                view, ctr, lane, nullptr, 0, &sq);
         if (LL) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);
@@ -307,8 +311,8 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
 // For K > kLargeK a sparse word's column is beta * r_k except at its own few topics, so its
 // statistics need no column: the top three come from its own topics and the first three
 // other topics of the CTA's list of topics in decreasing beta * r_k (ties to the lower k),
-// and the Q partials from one pass forming each phi_k as build_column does.  Dense words
-// keep k_word_stats.
+// and its split Q from its own entries and the smoothing table (Qw in st_ql slot 0, Qs in
+// slot 1).  Dense words keep k_word_stats.
 constexpr int kOrderList = 64;
 
 // (v, k) ranks above (a, i): larger value, ties to the lower topic.
@@ -328,7 +332,7 @@ __device__ __forceinline__ void top3_insert(float v, int k, float& a1, int& i1, 
 }
 
 __host__ __device__ __forceinline__ size_t stats_sparse_smem(int K, int warps) {
-    return (size_t)K * 4 + kOrderList * 4 + (size_t)warps * (large_bit_words(K) * 4 + large_pre_words(K) * 2);
+    return (size_t)K * 4 + kOrderList * 4 + (size_t)warps * (large_bit_words(K) * 4);
 }
 
 __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
@@ -336,12 +340,10 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
     __shared__ float red_v[8];
     __shared__ int red_k[8];
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bw = large_bit_words(a.K), pw = large_pre_words(a.K);
+    const int bw = large_bit_words(a.K);
     float* r = smf;
     int* order = reinterpret_cast<int*>(smf + a.K);
     uint32_t* bits = reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * wid;
-    uint16_t* pre = reinterpret_cast<uint16_t*>(reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * warps) +
-                    (size_t)pw * wid;
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     for (int i = lane; i < bw; i += 32) bits[i] = 0u;
     __syncthreads();
@@ -424,45 +426,48 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
             }
         }
         const int k1 = kk[0];
-        // prefix popcounts for the rank of a topic among the word's entries
-        uint32_t carry = 0;
-        for (int wb = 0; wb < bw; wb += 32) {
-            const int i = wb + lane;
-            const uint32_t c = i < bw ? (uint32_t)__popc(bits[i]) : 0u;
-            uint32_t incl = c;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t t = __shfl_up_sync(FULL, incl, off);
-                if (lane >= off) incl += t;
+        // Q = Qw + Qs (the split Q bucket): Qw over the word's own topics in rounds of 32
+        // entries (ascending k, the max topic's term 0), Qs = T[K-1] - sm_max
+        float carry = 0.0f;
+        for (uint32_t base = 0; base < nnz; base += 32) {
+            const uint32_t e = base + (uint32_t)lane;
+            float term = 0.0f;
+            if (e < nnz) {
+                const uint32_t en = __ldg(ent + e);
+                const int k = (int)(en >> 16);
+                if (k != k1) term = fmul(a.alpha, fmul(u2f(en & 0xffffu), r[k]));
             }
-            if (i < bw) pre[i] = (uint16_t)(carry + incl - c);
-            carry += __shfl_sync(FULL, incl, 31);
+            const float P = fadd(carry, warp_ks_scan(term, lane));
+            carry = __shfl_sync(FULL, P, 31);
         }
-        __syncwarp();
-        float ql = 0.0f;
-        for (int k = lane; k < a.K; k += 32) {
-            if (k == k1) continue;
-            const uint32_t bword = bits[k >> 5], m = 1u << (k & 31);
-            float phi;
-            if (bword & m) {
-                const uint32_t en = __ldg(ent + pre[k >> 5] + __popc(bword & (m - 1u)));
-                phi = fmul(fadd(u2f(en & 0xffffu), a.beta), r[k]);
-            } else {
-                phi = fmul(a.beta, r[k]);
-            }
-            ql = ffma(a.alpha, phi, ql);
-        }
-        const float qp = warp_ks_scan(ql, lane);
-        const float Q = __shfl_sync(FULL, qp, 31);
-        a.st_ql[(size_t)w * 32 + lane] = ql;
+        const float Qw = carry;
+        const float Qs = fsub(__ldg(a.smooth + a.K - 1), fmul(a.alpha, fmul(a.beta, r[k1])));
+        a.st_ql[(size_t)w * 32 + lane] = lane == 0 ? Qw : (lane == 1 ? Qs : 0.0f);
         if (lane == 0) {
             a.st_top2[w] = ((uint32_t)kk[1] << 16) | (uint32_t)k1;
             a.st_k3[w] = (uint32_t)kk[2];
-            a.st_phi[w] = make_float4(v[0], v[1], v[2], Q);
+            a.st_phi[w] = make_float4(v[0], v[1], v[2], fadd(Qw, Qs));
         }
         __syncwarp();
         for (uint32_t e = lane; e < nnz; e += 32) bits[(__ldg(ent + e) >> 16) >> 5] = 0u;
         __syncwarp();
+    }
+}
+
+// The smoothing table of the split Q bucket (K > kLargeK): T[k] = carry + Kogge-Stone scan
+// of sm_k = alpha * (beta * r_k) over rounds of 32 topics, the carry being the previous
+// round's last prefix, so T is non-decreasing and T[K-1] is the total.  One warp; r_k is
+// formed from n_k as fill_recip forms it.
+__global__ void __launch_bounds__(32) k_smooth_table(const int* __restrict__ n_k, int K, float Vbeta, float alpha,
+                                                     float beta, float* __restrict__ T) {
+    const int lane = threadIdx.x;
+    float carry = 0.0f;
+    for (int base = 0; base < K; base += 32) {
+        const int k = base + lane;
+        const float sm = k < K ? fmul(alpha, fmul(beta, __fdiv_rn(1.0f, fadd(__int2float_rn(n_k[k]), Vbeta)))) : 0.0f;
+        const float P = fadd(carry, warp_ks_scan(sm, lane));
+        if (k < K) T[k] = P;
+        carry = __shfl_sync(FULL, P, 31);
     }
 }
 

@@ -68,6 +68,27 @@ __global__ void __launch_bounds__(256) k_phi_dense(PhiArgs a) {
     }
 }
 
+// Above kLargeK topics the trainer's statistics give a sparse word its split Q bucket
+// ({Qw, Qs} in the lane-partial slots); the frozen model has no sparse word rows, so its
+// sparse words get the lane partials back, formed from the dense phi rows as k_word_stats
+// forms them from a column (serial fmaf of alpha * phi_k over k = l, l+32, ..., k != max),
+// with Q their Kogge-Stone total.  Warp per word.
+__global__ void __launch_bounds__(256) k_model_lane_q(int V, int Vd, int K, float alpha, const float* __restrict__ phi,
+                                                      const uint32_t* __restrict__ top2, float* __restrict__ ql,
+                                                      float4* __restrict__ phi4) {
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int w = Vd + blockIdx.x * warps + wid; w < V; w += gridDim.x * warps) {
+        const int k1 = (int)(__ldg(top2 + w) & 0xffffu);
+        const float* row = phi + (size_t)w * K;
+        float acc = 0.0f;
+        for (int k = lane; k < K; k += 32)
+            if (k != k1) acc = ffma(alpha, __ldg(row + k), acc);
+        const float Q = __shfl_sync(FULL, warp_ks_scan(acc, lane), 31);
+        ql[(size_t)w * 32 + lane] = acc;
+        if (lane == 0) phi4[w].w = Q;
+    }
+}
+
 // One active request of a step: its tokens sit at [tok_off, tok_off+len) of the pool and
 // it is split into items of `item_tokens` tokens, one warp each.  flags: FOLD_INIT (sweep
 // 0: sweep-start counts from the Philox initial topics), FOLD_LAST (the last sweep:
@@ -115,23 +136,24 @@ __device__ __forceinline__ float colz_of(const float* __restrict__ prow, int mk,
 
 // Serial fmaf chain over the lane's entries l, l + 32, ... of the document row (in shared
 // memory, so a step's 32 reads are conflict-free) with phi gathered from the frozen
-// matrix; the gathers of four entries are issued before their products are summed.
+// matrix.  The gathers of up to four entries are issued before their products are summed,
+// also when the lane has fewer than four left (rows of short requests hold only a few
+// entries per lane).
 __device__ __forceinline__ float fold_lane_mass(const uint32_t* row, uint32_t lane, uint32_t nnz,
                                                 const float* __restrict__ prow, int mk) {
     float acc = 0.0f;
-    uint32_t q = lane;
-    for (; q + 96u < nnz; q += 128u) {
-        const uint32_t e0 = row[q], e1 = row[q + 32u], e2 = row[q + 64u], e3 = row[q + 96u];
-        const float c0 = colz_of(prow, mk, e0 >> 16), c1 = colz_of(prow, mk, e1 >> 16);
-        const float c2 = colz_of(prow, mk, e2 >> 16), c3 = colz_of(prow, mk, e3 >> 16);
-        acc = ffma(u2f(e0 & 0xffffu), c0, acc);
-        acc = ffma(u2f(e1 & 0xffffu), c1, acc);
-        acc = ffma(u2f(e2 & 0xffffu), c2, acc);
-        acc = ffma(u2f(e3 & 0xffffu), c3, acc);
-    }
-    for (; q < nnz; q += 32u) {
-        const uint32_t e = row[q];
-        acc = ffma(u2f(e & 0xffffu), colz_of(prow, mk, e >> 16), acc);
+    for (uint32_t q = lane; q < nnz; q += 128u) {
+        uint32_t e[4];
+        float c[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const uint32_t i = q + 32u * j;
+            e[j] = i < nnz ? row[i] : 0u;
+            c[j] = i < nnz ? colz_of(prow, mk, e[j] >> 16) : 0.0f;
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            if (q + 32u * j < nnz) acc = ffma(u2f(e[j] & 0xffffu), c[j], acc);
     }
     return acc;
 }
@@ -143,31 +165,23 @@ __device__ __forceinline__ int fold_lane_draw(const uint32_t* row, uint32_t ls, 
                                               const float* __restrict__ prow, int mk, float t2) {
     float acc = 0.0f;
     int last = -1;
-    uint32_t q = ls;
-    for (; q + 96u < nnz; q += 128u) {
+    for (uint32_t q = ls; q < nnz; q += 128u) {
         uint32_t e[4];
         float c[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            e[j] = row[q + 32u * j];
-            c[j] = colz_of(prow, mk, e[j] >> 16);
+            const uint32_t i = q + 32u * j;
+            e[j] = i < nnz ? row[i] : 0u;
+            c[j] = i < nnz ? colz_of(prow, mk, e[j] >> 16) : 0.0f;
         }
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
+            if (q + 32u * j >= nnz) break;
             acc = ffma(u2f(e[j] & 0xffffu), c[j], acc);
             if (c[j] > 0.0f) {
                 last = (int)(e[j] >> 16);
                 if (t2 < acc) return last;
             }
-        }
-    }
-    for (; q < nnz; q += 32u) {
-        const uint32_t e = row[q];
-        const float cz = colz_of(prow, mk, e >> 16);
-        acc = ffma(u2f(e & 0xffffu), cz, acc);
-        if (cz > 0.0f) {
-            last = (int)(e >> 16);
-            if (t2 < acc) return last;
         }
     }
     return last >= 0 ? last : mk;
@@ -422,6 +436,12 @@ extern "C" int lda_model_from_trainer(lda_trainer* t, int64_t device_budget, lda
     CUDA_TRY(cudaMemcpyAsync(m->top2, src.top2, sizeof(uint32_t) * (size_t)m->V, cudaMemcpyDeviceToDevice, stream));
     CUDA_TRY(cudaMemcpyAsync(m->phi4, src.phi4, sizeof(float4) * (size_t)m->V, cudaMemcpyDeviceToDevice, stream));
     CUDA_TRY(cudaMemcpyAsync(m->ql, src.ql, sizeof(float) * 32 * (size_t)m->V, cudaMemcpyDeviceToDevice, stream));
+    if (m->K > dev::kLargeK && m->V > src.Vd) {
+        const int grid = (int)std::min<int64_t>(4096, (m->V - src.Vd + 7) / 8);
+        dev::k_model_lane_q<<<grid, 256, 0, stream>>>((int)m->V, src.Vd, m->K, m->alpha, m->phi, m->top2, m->ql,
+                                                      reinterpret_cast<float4*>(m->phi4));
+        CUDA_TRY(cudaGetLastError());
+    }
     CUDA_TRY(cudaStreamSynchronize(stream));
     *out = m.release();
     return LDA_OK;

@@ -132,6 +132,7 @@ struct StatsArgs {
     uint32_t* st_k3;
     float4* st_phi;     // {phi_max, phi_2nd, phi_3rd, Q}
     float* st_ql;       // [V*32]
+    const float* smooth = nullptr;  // K > kLargeK: the smoothing table (k_smooth_table)
 };
 
 // Statistics of word w from its column (built into the warp's shared `col`).
@@ -285,7 +286,8 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& his
         while (m) {
             const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
             m &= m - 1u;
-            out[p++] = (k << 16) | hist.get(k);
+            const uint32_t key = a.K <= kLargeK ? (uint32_t)col_skew((int)k) : k;
+            out[p++] = (key << 16) | hist.get(k);
             hist.clear(k);
         }
     }
@@ -341,11 +343,48 @@ struct SampleArgs {
     // r_k = 1 / ((float)n_k + V*beta) for k < K, formed once per sweep (the K > kLargeK
     // dense-word sampler reads it instead of dividing for every tile's column)
     const float* recip = nullptr;
+    // K > kLargeK: the smoothing table of the split Q bucket (k_smooth_table)
+    const float* smooth = nullptr;
 };
 
-// Above this many topics the trainer samples with the CTA-per-tile dense-word kernel and
-// the column-free sparse-word kernel (kernels.cuh) instead of a column per warp.
-constexpr int kLargeK = 2048;
+// The split Q bucket of a sparse word above kLargeK topics: Q = Qw + Qs, Qw over the word's
+// own topics, Qs the word-independent smoothing part alpha * beta * sum_{k != max} r_k.
+struct SplitQ {
+    const uint32_t* ent;  // the word's row (k << 16 | count), ascending k
+    uint32_t nnz;
+    float Qw;
+    const float* T;       // the smoothing table (K entries, non-decreasing)
+    const float* r;       // r_k, at col_skew(k) when skew
+    bool skew;
+    __device__ __forceinline__ float rk(int k) const { return r[skew ? col_skew(k) : k]; }
+};
+
+// The Q-bucket draw of a split word for t = target - pS (uniform across the warp): the
+// word's own topics first, in rounds of 32 entries (carry + Kogge-Stone scan of
+// alpha * (n_wk * r_k), the max topic's term 0; the first entry with a non-zero term whose
+// prefix exceeds t, else the last such entry); otherwise smoothing for t' = t - Qw against
+// T with the max topic left out: the first k < maxK with t' < T[k] when t' < T[maxK-1],
+// else the first k > maxK with t' + sm_max < T[k], else the last topic other than maxK.
+__device__ __forceinline__ int split_q_draw(const SplitQ& q, float t, int maxK, int K, float alpha, float beta,
+                                            int lane) {
+    if (t < q.Qw) {
+        auto slot = [&](uint32_t i, int& key, float& term, bool& ok) {
+            const uint32_t en = __ldg(q.ent + i);
+            const int k = (int)(en >> 16);
+            term = k == maxK ? 0.0f : fmul(alpha, fmul(u2f(en & 0xffffu), q.rk(k)));
+            key = k;
+            ok = term > 0.0f;
+        };
+        const int z = warp_level2(q.nnz, t, -1, lane, slot);
+        if (z >= 0) return z;
+    }
+    const float t1 = fsub(t, q.Qw);
+    if (maxK > 0 && t1 < __ldg(q.T + maxK - 1)) return warp_first_above(q.T, 0, maxK, t1, lane);
+    const float t2 = fadd(t1, fmul(alpha, fmul(beta, q.rk(maxK))));
+    const int z = warp_first_above(q.T, maxK + 1, K, t2, lane);
+    return z >= 0 ? z : (maxK == K - 1 ? K - 2 : K - 1);
+}
+
 
 // Sweep counters live in shared memory (one row per warp, written by lane 0) so they
 // cost no registers in the sampling loop.
@@ -372,18 +411,27 @@ constexpr int kSampleWarps = LDA_SAMPLE_WARPS;
 #define LDA_SPARSE_LARGE_MIN_BLOCKS 4
 #endif
 
+#ifndef LDA_ROW_PREFETCH
+#define LDA_ROW_PREFETCH 0
+#endif
+
 // Branch taken by a token (counters only).
 enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 
 // The 32-token groups g0, g0 + gstep, ... of the token range [start, start + cnt) of one
 // word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word).
 // Returns the lane's LL partial (LL mode).
-template <bool LL, int QB, class View>
+template <bool LL, int QB, bool SPLIT = false, class View>
 __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t start, uint32_t cnt, uint32_t g0,
                                                 uint32_t gstep, uint32_t iter, int maxK, const float4 ph, float QL,
                                                 float QP, float Q, const View& colz, uint32_t* ctr, int lane,
-                                                const float2* qtab = nullptr, int qrounds = 0) {
+                                                const float2* qtab = nullptr, int qrounds = 0,
+                                                const SplitQ* sq = nullptr) {
     double ll = 0.0;
+    // LL mode: the lane's factors total_t and (n_d + K alpha) as FP64 products, one log of
+    // their ratio per 16 tokens (earlier if a product leaves [1e-150, 1e150])
+    double ll_num = 1.0, ll_den = 1.0;
+    int ll_n = 0;
     uint32_t cur = 0xffffffffu, nnz = 0;
     const uint32_t* row = a.dt_ent;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
@@ -417,9 +465,46 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
         const unsigned emask = __ballot_sync(FULL, ea);
         const unsigned need0 = LL ? vmask : (vmask & ~emask);
         unsigned need = need0;
+#if LDA_ROW_PREFETCH
+        // the needed tokens that start a new row: the first whose doc differs from `cur`,
+        // then each whose doc differs from the previous needed token's
+        const unsigned below = need0 & ((1u << lane) - 1u);
+        const uint32_t dprev = __shfl_sync(FULL, d, below ? 31 - __clz(below) : lane);
+        const bool newrow = ((need0 >> lane) & 1u) && d != (below ? dprev : cur);
+        unsigned rows = __ballot_sync(FULL, newrow);
+        evaluated = newrow;
+        if (need0) cur = __shfl_sync(FULL, d, 31 - __clz(need0));
+        // the first two steps of the next row to evaluate are loaded one row ahead
+        uint32_t pf_nnz = 0, pf_off = 0, pf0 = 0, pf1 = 0;
+        auto prefetch = [&](unsigned rest) {
+            if (rest) {
+                const int j2 = __ffs(rest) - 1;
+                pf_nnz = __shfl_sync(FULL, my_nnz, j2);
+                pf_off = __shfl_sync(FULL, my_off, j2);
+                const uint32_t* r2 = a.dt_ent + pf_off;
+                pf0 = (uint32_t)lane < pf_nnz ? __ldg(r2 + lane) : 0u;
+                pf1 = (uint32_t)lane + 32u < pf_nnz ? __ldg(r2 + lane + 32) : 0u;
+            }
+        };
+        prefetch(rows);
+#endif
         while (need) {
             const int j = __ffs(need) - 1;
             need &= need - 1u;
+#if LDA_ROW_PREFETCH
+            if ((rows >> j) & 1u) {
+                nnz = pf_nnz;
+                row = a.dt_ent + pf_off;
+                const uint32_t e0 = pf0, e1 = pf1;
+                prefetch(j == 31 ? 0u : rows & (0xfffffffeu << j));
+                float acc = 0.0f;
+                if ((uint32_t)lane < nnz) acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
+                if ((uint32_t)lane + 32u < nnz) acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
+                SL = lane_mass(row, (uint32_t)lane + 64u, nnz, colz, acc);
+                SP = warp_ks_scan(SL, lane);
+                S = __shfl_sync(FULL, SP, 31);
+            }
+#else
             const uint32_t dj = __shfl_sync(FULL, d, j);
             if (dj != cur) {
                 cur = dj;
@@ -430,6 +515,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 S = __shfl_sync(FULL, SP, 31);
                 evaluated |= (lane == j);
             }
+#endif
             const float pmj = __shfl_sync(FULL, pmax, j);
             const float uj = __shfl_sync(FULL, u, j);
             const float pS = fadd(pmj, S);
@@ -454,32 +540,45 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 }
             } else {
                 const float tt = fsub(target, pS);
-                const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
-                const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
-                const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
-                const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
-                const float t2 = ls > 0 ? fsub(tt, prev) : tt;
-                const int K = a.K;
-                const float alpha = a.alpha;
-                const uint32_t n = (uint32_t)((K - ls + 31) / 32);
-                auto slot = [&](uint32_t i, int& key, float& term, bool& ok) {
-                    const int k = ls + 32 * (int)i;
-                    const float cz = colz(k);
-                    key = k;
-                    term = fmul(alpha, cz);
-                    ok = cz > 0.0f;
-                };
-                int zq = qtab ? warp_level2_table(n, t2, lane, slot, qtab + ls * qrounds) : -1;
-                if (zq < 0) zq = warp_level2_rounds<QB>(n, t2, maxK, lane, slot);
+                int zq;
+                if (SPLIT) {
+                    zq = split_q_draw(*sq, tt, maxK, a.K, a.alpha, a.beta, lane);
+                } else {
+                    const unsigned cand = __ballot_sync(FULL, tt < QP && QL > 0.0f);
+                    const unsigned pos = __ballot_sync(FULL, QL > 0.0f);
+                    const int ls = cand ? __ffs(cand) - 1 : (pos ? 31 - __clz(pos) : 0);
+                    const float prev = __shfl_sync(FULL, QP, ls > 0 ? ls - 1 : 0);
+                    const float t2 = ls > 0 ? fsub(tt, prev) : tt;
+                    const int K = a.K;
+                    const float alpha = a.alpha;
+                    const uint32_t n = (uint32_t)((K - ls + 31) / 32);
+                    auto slot = [&](uint32_t i, int& key, float& term, bool& ok) {
+                        const int k = ls + 32 * (int)i;
+                        const float cz = colz(k);
+                        key = k;
+                        term = fmul(alpha, cz);
+                        ok = cz > 0.0f;
+                    };
+                    zq = qtab ? warp_level2_table(n, t2, lane, slot, qtab + ls * qrounds) : -1;
+                    if (zq < 0) zq = warp_level2_rounds<QB>(n, t2, maxK, lane, slot);
+                }
                 if (lane == j) {
                     kind = BR_Q;
                     znew = zq;
                 }
             }
         }
-        // each lane's own token's log-likelihood term, all lanes at once (every lane
+        // each lane's own token's log-likelihood factors, all lanes at once (every lane
         // accumulates only its own tokens, in group order)
-        if (LL && valid) ll += log((double)my_total / ((double)nd + a.den_add));
+        if (LL && valid) {
+            ll_num *= (double)my_total;
+            ll_den *= (double)nd + a.den_add;
+            if (++ll_n == 16 || ll_num < 1e-150 || ll_num > 1e150 || ll_den > 1e150) {
+                ll += log(ll_num / ll_den);
+                ll_num = ll_den = 1.0;
+                ll_n = 0;
+            }
+        }
         if (kind == BR_S) znew = lane_draw(my_row, my_ls, my_nnz_s, colz, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
@@ -500,6 +599,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
             ctr[C_RENT] += nnz_rows;
         }
     }
+    if (LL && ll_n) ll += log(ll_num / ll_den);
     return ll;
 }
 
@@ -507,9 +607,10 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
 // warp's shared `col` (col_words(K) floats, skewed layout), the reciprocal table `r` and
 // the warp's shared counter row `ctr`.  QB: Q-bucket rounds decided per batch (1 for
 // K <= 1024, where a lane has one round of topics).
-template <bool LL, int QB = 1>
+template <bool LL, int QB = 1, bool SKEWKEYS = true>
 __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const int4 t, uint32_t iter,
                                             const float* r, float* col, uint32_t* ctr, int lane) {
+    using View = ColSharedT<SKEWKEYS>;
     const int w = t.x;
     const uint32_t start = (uint32_t)t.y, cnt = (uint32_t)t.z;
     __syncwarp();
@@ -526,7 +627,21 @@ __device__ __forceinline__ void sample_tile(const SampleArgs& a, int tile, const
     const float Q = __shfl_sync(FULL, QP, 31);
     if (lane == 0) col[col_skew(maxK)] = 0.0f;
     __syncwarp();
-    double ll = sample_groups<LL, QB>(a, start, cnt, 0u, 32u, iter, maxK, ph, QL, QP, Q, ColShared{col}, ctr, lane);
+    double ll;
+    if constexpr (QB > 1) {
+        if (a.K > kLargeK && w >= a.Vd) {
+            // a sparse word above kLargeK topics: the split Q bucket
+            const int s = w - a.Vd;
+            const SplitQ sq{a.swt_ent + __ldg(a.swt_off + s), __ldg(a.swt_nnz + s), __shfl_sync(FULL, QL, 0),
+                            a.smooth, r, false};
+            ll = sample_groups<LL, QB, true>(a, start, cnt, 0u, 32u, iter, maxK, ph, QL, QP, Q, View{col}, ctr,
+                                             lane, nullptr, 0, &sq);
+        } else {
+            ll = sample_groups<LL, QB>(a, start, cnt, 0u, 32u, iter, maxK, ph, QL, QP, Q, View{col}, ctr, lane);
+        }
+    } else {
+        ll = sample_groups<LL, QB>(a, start, cnt, 0u, 32u, iter, maxK, ph, QL, QP, Q, View{col}, ctr, lane);
+    }
     if (LL) {
 #pragma unroll
         for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);

@@ -53,6 +53,7 @@ struct lda_trainer {
     int K = 0, Vd = 0, C = 0, warps = 8, num_sms = 0;
     int swarps = 8;  // warps per CTA of the K <= 2048 sampler
     float* recip = nullptr;  // [K] per-sweep reciprocals (K > kLargeK)
+    float* smooth = nullptr; // [K] per-sweep smoothing table of the split Q bucket (K > kLargeK)
     int warps_wt = 8, warps_dt = 8;  // warps per CTA of the word-topic and doc-topic rebuilds
     float alpha = 0, beta = 0, Vbeta = 0;
     uint64_t seed = 0;
@@ -262,9 +263,15 @@ static int occupancy_grid(const void* fn, int threads, size_t smem, int num_sms,
 // several rounds, which are decided four per batch.
 static int sample_qb(int K) { return K > 1024 ? 4 : 1; }
 
-static const void* sample_kernel(bool ll, int K) {
-    if (sample_qb(K) == 4) return ll ? (const void*)dev::k_sample_t<true, 4> : (const void*)dev::k_sample_t<false, 4>;
-    return ll ? (const void*)dev::k_sample_t<true, 1> : (const void*)dev::k_sample_t<false, 1>;
+// skew: the doc rows' keys are word-column slot indices (the trainer's own rows); the
+// allocation-free entry point samples rows whose keys are topics.
+static const void* sample_kernel(bool ll, int K, bool skew = true) {
+    if (sample_qb(K) == 4) {
+        if (skew) return ll ? (const void*)dev::k_sample_t<true, 4, true> : (const void*)dev::k_sample_t<false, 4, true>;
+        return ll ? (const void*)dev::k_sample_t<true, 4, false> : (const void*)dev::k_sample_t<false, 4, false>;
+    }
+    if (skew) return ll ? (const void*)dev::k_sample_t<true, 1, true> : (const void*)dev::k_sample_t<false, 1, true>;
+    return ll ? (const void*)dev::k_sample_t<true, 1, false> : (const void*)dev::k_sample_t<false, 1, false>;
 }
 
 // K > kLargeK: the dense-word (CTA per tile) and sparse-word (no column) samplers; a lane's
@@ -276,13 +283,24 @@ static const void* sparse_large_kernel(bool ll) {
     return ll ? (const void*)dev::k_sample_sparse_large<true, 4> : (const void*)dev::k_sample_sparse_large<false, 4>;
 }
 
-static void launch_sample(bool ll, int K, int grid, int threads, size_t smem, cudaStream_t q, const dev::SampleArgs& a) {
+static void launch_sample(bool ll, int K, int grid, int threads, size_t smem, cudaStream_t q, const dev::SampleArgs& a,
+                          bool skew = true) {
     if (sample_qb(K) == 4) {
-        if (ll) dev::k_sample_t<true, 4><<<grid, threads, smem, q>>>(a);
-        else dev::k_sample_t<false, 4><<<grid, threads, smem, q>>>(a);
+        if (skew) {
+            if (ll) dev::k_sample_t<true, 4, true><<<grid, threads, smem, q>>>(a);
+            else dev::k_sample_t<false, 4, true><<<grid, threads, smem, q>>>(a);
+        } else {
+            if (ll) dev::k_sample_t<true, 4, false><<<grid, threads, smem, q>>>(a);
+            else dev::k_sample_t<false, 4, false><<<grid, threads, smem, q>>>(a);
+        }
     } else {
-        if (ll) dev::k_sample_t<true, 1><<<grid, threads, smem, q>>>(a);
-        else dev::k_sample_t<false, 1><<<grid, threads, smem, q>>>(a);
+        if (skew) {
+            if (ll) dev::k_sample_t<true, 1, true><<<grid, threads, smem, q>>>(a);
+            else dev::k_sample_t<false, 1, true><<<grid, threads, smem, q>>>(a);
+        } else {
+            if (ll) dev::k_sample_t<true, 1, false><<<grid, threads, smem, q>>>(a);
+            else dev::k_sample_t<false, 1, false><<<grid, threads, smem, q>>>(a);
+        }
     }
 }
 
@@ -500,7 +518,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
     ALLOC(T.tile_ctr, 1 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
-    if (T.large) ALLOC(T.recip, T.K);
+    if (T.large) { ALLOC(T.recip, T.K); ALLOC(T.smooth, T.K); }
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
 
@@ -649,6 +667,7 @@ static dev::StatsArgs stats_args(const lda_trainer* t) {
     a.V = (int)t->V; a.Vd = t->Vd; a.K = t->K; a.alpha = t->alpha; a.beta = t->beta; a.Vbeta = t->Vbeta;
     a.n_k = t->n_k; a.dwt = t->dwt; a.swt_off = t->swt_off; a.swt_nnz = t->swt_nnz; a.swt_ent = t->swt_ent;
     a.st_top2 = t->st_top2; a.st_k3 = t->st_k3; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
+    a.smooth = t->smooth;
     return a;
 }
 
@@ -676,7 +695,10 @@ extern "C" int lda_max_topic(lda_trainer* t) {
         dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
         CUDA_TRY(cudaGetLastError());
     } else {
-        // dense words from their columns, sparse words without one
+        // the smoothing table of the sparse words' split Q bucket, then dense words from
+        // their columns, sparse words without one
+        dev::k_smooth_table<<<1, 32, 0, t->stream>>>(t->n_k, t->K, t->Vbeta, t->alpha, t->beta, t->smooth);
+        CUDA_TRY(cudaGetLastError());
         if (t->Vd > 0) {
             dev::StatsArgs ad = a;
             ad.V = t->Vd;
@@ -771,6 +793,7 @@ static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, in
     a.st_top2 = t->st_top2; a.st_phi = t->st_phi; a.st_ql = t->st_ql;
     a.tok_doc = b.tok_doc; a.meta = b.meta; a.z = t->z; a.doc_len = t->doc_len;
     a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.ctr = t->ctr;
+    a.smooth = t->smooth;
     a.tok_base = b.tok_base;
     a.dt_base = b.dt_base;
     a.recip = t->recip;
@@ -1366,7 +1389,13 @@ extern "C" int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent,
     for (int64_t d = 0; d < t->D; ++d) {
         if (ent) {
             if (n + hnnz[d] > cap) return fail(LDA_ERR_ARG, "doc-row buffer too small");
-            std::memcpy(ent + n, hent.data() + hoff[d], sizeof(uint32_t) * hnnz[d]);
+            const uint32_t* src = hent.data() + hoff[d];
+            for (uint32_t j = 0; j < hnnz[d]; ++j) {
+                // up to kLargeK topics the device rows carry word-column slot indices
+                const uint32_t key = src[j] >> 16;
+                const uint32_t k = t->K <= dev::kLargeK ? (uint32_t)dev::col_unskew((int)key) : key;
+                ent[n + j] = (k << 16) | (src[j] & 0xffffu);
+            }
         }
         n += hnnz[d];
         off[d + 1] = n;
@@ -1388,13 +1417,17 @@ extern "C" int lda_get_token_meta(lda_trainer* t, uint32_t* meta) {
 // lda_sample_chunk_noalloc runs the same k_sample / k_ll_reduce kernels on buffers the
 // caller owns.  Its scratch lives in one file-scope device array: bytes [0,4) the tile
 // counter, [8,136) the sweep counters, [256, 256 + 8*kNoAllocMaxTiles) the per-tile LL
-// partials.  In host code the symbol is only a host-side stand-in, so the device address
+// partials, then (K > 2048) the smoothing table of the split Q bucket, K floats.  In host code the symbol is only a host-side stand-in, so the device address
 // is looked up once per device (with that device current) and cached.
 
 namespace {
 constexpr int kNoAllocMaxTiles = 65536;
 constexpr size_t kNoAllocHeader = 256;
-constexpr size_t kNoAllocBytes = kNoAllocHeader + sizeof(double) * (size_t)kNoAllocMaxTiles;
+// above 2048 topics the split Q bucket's smoothing table (K floats) follows the LL partials;
+// K is bounded below this by the sampler's shared memory anyway
+constexpr int kNoAllocMaxK = 29696;
+constexpr size_t kNoAllocSmooth = kNoAllocHeader + sizeof(double) * (size_t)kNoAllocMaxTiles;
+constexpr size_t kNoAllocBytes = kNoAllocSmooth + sizeof(float) * (size_t)kNoAllocMaxK;
 constexpr int kMaxDevices = 64;
 std::mutex g_noalloc_mu;
 unsigned char* g_noalloc_addr[kMaxDevices] = {};
@@ -1485,7 +1518,8 @@ static int noalloc_scratch(int device, unsigned char** out) {
 
 extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device, void* stream_ptr) {
     if (!io) return fail(LDA_ERR_ARG, "null io");
-    if (io->K < 4 || io->K > 65535) return fail(LDA_ERR_ARG, "K=%d outside [4, 65535]", io->K);
+    if (io->K < 4 || io->K > kNoAllocMaxK)
+        return fail(LDA_ERR_ARG, "K=%d outside [4, %d] (the allocation-free limit)", io->K, kNoAllocMaxK);
     if (io->num_tiles < 0 || io->num_tiles > kNoAllocMaxTiles)
         return fail(LDA_ERR_ARG, "num_tiles=%d exceeds the allocation-free limit of %d tiles per call",
                     io->num_tiles, kNoAllocMaxTiles);
@@ -1527,7 +1561,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     if (warps < 1) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
     const size_t smem = (size_t)io->K * 4 + (size_t)warps * (dev::col_words(io->K) * 4 + 16 * sizeof(uint32_t));
     if (warps < 1 || smem > (size_t)max_smem) return fail(LDA_ERR_ARG, "K=%d does not fit in shared memory", io->K);
-    const void* kfn = sample_kernel(io->ll_mode != 0, io->K);
+    const void* kfn = sample_kernel(io->ll_mode != 0, io->K, false);
     CUDA_TRY(raise_smem_limit(kfn, smem));
     int grid = 0;
     if ((rc = occupancy_grid(kfn, 32 * warps, smem, num_sms, &grid))) return rc;
@@ -1549,6 +1583,12 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.ctr = reinterpret_cast<unsigned long long*>(scratch + 8);
     a.tok_base = 0;
     a.dt_base = 0;
+    if (io->K > dev::kLargeK) {
+        a.smooth = reinterpret_cast<const float*>(scratch + kNoAllocSmooth);
+        dev::k_smooth_table<<<1, 32, 0, st>>>(io->n_k, io->K, a.Vbeta, io->alpha, io->beta,
+                                              reinterpret_cast<float*>(scratch + kNoAllocSmooth));
+        CUDA_TRY(cudaGetLastError());
+    }
     IoCheck chk;
     chk.tiles = a.tiles; chk.ntiles = io->num_tiles; chk.K = io->K; chk.V = io->vocab; chk.Vd = io->num_dense;
     chk.D = io->num_docs; chk.top2 = io->top2; chk.swt_off = io->sparse_off; chk.swt_nnz = io->sparse_nnz;
@@ -1557,7 +1597,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     chk.n_sp = io->num_sparse_entries; chk.status = io->status; chk.tile_counter = a.tile_counter;
     k_check_sample_io<<<4 * num_sms, 256, 0, st>>>(chk);
     CUDA_TRY(cudaGetLastError());
-    launch_sample(a.ll_mode != 0, io->K, grid, 32 * warps, smem, st, a);
+    launch_sample(a.ll_mode != 0, io->K, grid, 32 * warps, smem, st, a, false);
     CUDA_TRY(cudaGetLastError());
     if (io->ll_mode) {
         dev::k_ll_reduce<<<1, 1024, 0, st>>>(a.tile_ll, io->num_tiles, io->ll_sum);

@@ -61,6 +61,7 @@ def lib() -> C.CDLL:
         L.orc_foldin_init.restype = C.c_uint16
         L.orc_get_phi_row.argtypes = [P, C.c_int32, P]
         L.orc_set_doc_range.argtypes = [P, C.c_int32, C.c_int32]
+        L.orc_set_num_dense.argtypes = [P, C.c_int32]
         _lib = L
     return _lib
 
@@ -81,7 +82,7 @@ class Oracle:
     """Serial/threaded restatement of one EZLDA sweep over a word-sorted corpus."""
 
     def __init__(self, tok_word, tok_doc, V: int, D: int, K: int, alpha: float, beta: float,
-                 nthreads: int = 0):
+                 nthreads: int = 0, num_dense: int = 0):
         self.tok_word = np.ascontiguousarray(tok_word, dtype=np.int32)
         self.tok_doc = np.ascontiguousarray(tok_doc, dtype=np.int32)
         self.N, self.V, self.D, self.K = len(self.tok_word), V, D, K
@@ -92,6 +93,8 @@ class Oracle:
                                    self.alpha, self.beta, nt)
         if not self._h:
             raise ValueError("orc_create rejected the corpus")
+        if lib().orc_set_num_dense(self._h, int(num_dense)):
+            raise ValueError(f"bad num_dense {num_dense}")
         self._z = None
 
     def close(self):

@@ -50,6 +50,17 @@
  *   with L[l] > 0); t2 = t - P[l-1].  In the lane: the first entry/slot with
  *   colz > 0 whose partial sum / prefix exceeds t2, else the last one with
  *   colz > 0, else maxK.
+ *   Split Q (K > 2048 and a sparse word, w >= Vd; SparseLDA's smoothing / word split):
+ *   sm_k    = alpha * (beta * r_k); T[k] = carry + Kogge-Stone scan of sm over rounds
+ *             of 32 topics (carry = the previous round's last prefix), Tsum = T[K-1]
+ *   Qw      = the same rounds over the word's own topics (ascending k) with terms
+ *             alpha * ((float)n_wk * r_k), the max topic's term 0; Qs = Tsum - sm_max;
+ *             Q = Qw + Qs (QL = {Qw, Qs, 0, ...})
+ *   Q draw  : t < Qw -> the first own topic with a non-zero term whose prefix exceeds t
+ *             (else the last such topic); otherwise t' = t - Qw: the first k < maxK with
+ *             t' < T[k] if t' < T[maxK-1], else the first k > maxK with t' + sm_max < T[k],
+ *             else the last topic other than maxK.  Fold-in keeps the lane form (its
+ *             frozen model has no word rows): QL from the column as above.
  *   LL_i    = log((double)total / ((double)n_d + (double)K * (double)alpha))
  * Randoms: u = (float)(x0 >> 8) * 2^-24 with x = Philox4x32-10(ctr = {tok_lo,
  * tok_hi, iter, 0x4C444131}, key = {seed_lo, seed_hi}); initial topic =
@@ -98,9 +109,16 @@ uint16_t orc_init_topic(uint64_t seed, uint64_t tok, int32_t K) {
 }
 
 /* ------------------------------------------------------------------- state */
+/* Above this many topics a sparse word (w >= Vd) splits its Q bucket into the word's own
+ * topics and a word-independent smoothing part (see the specification above). */
+#define ORC_LARGE_K 2048
+
 struct orc_state {
     int64_t N;
     int32_t doc_lo, doc_hi; /* orc_sample draws only tokens of docs in [doc_lo, doc_hi) */
+    int32_t Vd;             /* words [0, Vd) are dense (the trainer's split) */
+    float* T;               /* K > ORC_LARGE_K: smoothing prefix table, T[K-1] = Tsum */
+    float Tsum;
     int32_t V, D, K, nthreads;
     float alpha, beta;
     const int32_t* tok_word;
@@ -152,6 +170,7 @@ orc_state* orc_create(int64_t N, int32_t V, int32_t D, int32_t K, const int32_t*
     s->alpha = alpha; s->beta = beta;
     s->tok_word = tok_word; s->tok_doc = tok_doc;
     s->doc_lo = 0; s->doc_hi = D;
+    s->Vd = 0;
     s->woff = counting_index(N, V, tok_word, &s->wtok);
     s->doff = counting_index(N, D, tok_doc, &s->dtok);
     s->rcap = (int64_t*)calloc((size_t)D + 1, sizeof(int64_t));
@@ -162,8 +181,9 @@ orc_state* orc_create(int64_t N, int32_t V, int32_t D, int32_t K, const int32_t*
     s->k3 = (uint32_t*)calloc((size_t)V, sizeof(uint32_t));
     s->phi4 = (float*)calloc((size_t)V * 4, sizeof(float));
     s->ql = (float*)calloc((size_t)V * LANES, sizeof(float));
+    s->T = (float*)calloc((size_t)K, sizeof(float));
     if (!s->woff || !s->doff || !s->rcap || !s->n_k || !s->r || !s->rnnz || !s->top2 || !s->k3 ||
-        !s->phi4 || !s->ql) {
+        !s->phi4 || !s->ql || !s->T) {
         orc_destroy(s);
         return NULL;
     }
@@ -181,9 +201,19 @@ void orc_destroy(orc_state* s) {
     if (!s) return;
     free(s->woff); free(s->wtok); free(s->doff); free(s->dtok); free(s->rcap);
     free(s->n_k); free(s->r); free(s->rnnz); free(s->rent);
-    free(s->top2); free(s->k3); free(s->phi4); free(s->ql);
+    free(s->top2); free(s->k3); free(s->phi4); free(s->ql); free(s->T);
     free(s);
 }
+
+int orc_set_num_dense(orc_state* s, int32_t Vd) {
+    if (!s || Vd < 0 || Vd > s->V) return -1;
+    s->Vd = Vd;
+    s->built = 0;
+    return 0;
+}
+
+/* Whether word w draws its Q bucket in two parts (the word's topics, then smoothing). */
+static int split_word(const orc_state* s, int32_t w) { return s->K > ORC_LARGE_K && w >= s->Vd; }
 
 /* ------------------------------------------------------------- thread pool */
 typedef void (*task_fn)(void* ctx, int64_t begin, int64_t end, int tid);
@@ -319,14 +349,37 @@ static void rb_word_stats(void* c, int64_t b, int64_t e, int tid) {
             if (m3 < 0 || col[k] > col[m3]) m3 = k;
         }
         float* ql = s->ql + w * LANES;
-        for (int l = 0; l < LANES; ++l) {
-            float acc = 0.0f;
-            for (int32_t k = l; k < K; k += LANES)
-                if (k != m1) acc = fmaf(s->alpha, col[k], acc);
-            ql[l] = acc;
-        }
         float qp[LANES];
-        ks_scan32(ql, qp);
+        if (split_word(s, (int32_t)w)) {
+            /* Q = Qw + Qs: Qw over the word's own topics in rounds of 32 entries (ascending
+             * k, the max topic's term 0), Qs = Tsum - sm_max; ql holds {Qw, Qs, 0, ...} */
+            float carry = 0.0f, tr[LANES], P[LANES];
+            int n = 0;
+            for (int32_t k = 0; k <= K; ++k) {
+                if (k < K) {
+                    if (!cnt[k]) continue;
+                    tr[n++] = k == m1 ? 0.0f : s->alpha * ((float)cnt[k] * s->r[k]);
+                }
+                if (n == LANES || (k == K && n > 0)) {
+                    for (int i = n; i < LANES; ++i) tr[i] = 0.0f;
+                    ks_scan32(tr, P);
+                    carry = carry + P[LANES - 1];
+                    n = 0;
+                }
+            }
+            memset(ql, 0, sizeof(float) * LANES);
+            ql[0] = carry;
+            ql[1] = s->Tsum - s->alpha * (s->beta * s->r[m1]);
+            qp[LANES - 1] = ql[0] + ql[1];
+        } else {
+            for (int l = 0; l < LANES; ++l) {
+                float acc = 0.0f;
+                for (int32_t k = l; k < K; k += LANES)
+                    if (k != m1) acc = fmaf(s->alpha, col[k], acc);
+                ql[l] = acc;
+            }
+            ks_scan32(ql, qp);
+        }
         s->top2[w] = ((uint32_t)m2 << 16) | (uint32_t)m1;
         s->k3[w] = (uint32_t)m3;
         s->phi4[w * 4 + 0] = col[m1];
@@ -360,6 +413,20 @@ int orc_rebuild(orc_state* s, const uint16_t* z) {
         for (int32_t k = 0; k < s->K; ++k) s->n_k[k] += x.nkp[t][k];
     const float Vb = (float)s->V * s->beta;
     for (int32_t k = 0; k < s->K; ++k) s->r[k] = 1.0f / ((float)s->n_k[k] + Vb);
+    if (s->K > ORC_LARGE_K) {
+        /* smoothing table: T[k] = carry + Kogge-Stone scan of sm in rounds of 32 topics,
+         * sm_k = alpha * (beta * r_k); the carry is the previous round's last prefix */
+        float carry = 0.0f;
+        for (int32_t base = 0; base < s->K; base += LANES) {
+            float tr[LANES], P[LANES];
+            for (int i = 0; i < LANES; ++i)
+                tr[i] = base + i < s->K ? s->alpha * (s->beta * s->r[base + i]) : 0.0f;
+            ks_scan32(tr, P);
+            for (int i = 0; i < LANES && base + i < s->K; ++i) s->T[base + i] = carry + P[i];
+            carry = carry + P[LANES - 1];
+        }
+        s->Tsum = carry;
+    }
     parallel_for(nt, s->D, 256, rb_doc_rows, &x);
     parallel_for(nt, s->V, 64, rb_word_stats, &x);
     for (int t = 0; t < nt; ++t) { free(x.icnt[t]); free(x.fcol[t]); free(x.list[t]); free(x.nkp[t]); }
@@ -492,7 +559,60 @@ typedef struct {
     const float* QL;   /* 32 lane partials of Q */
     const float* QP;   /* their Kogge-Stone scan */
     const float* colz; /* the word's column with colz[maxK] = 0 */
+    /* split Q (K > ORC_LARGE_K, sparse word): Q = Qw + Qs */
+    int split;
+    float Qw, Qs, beta, Tsum;
+    const int32_t* wk; /* the word's topics, ascending */
+    const int32_t* wn; /* their counts */
+    int32_t nw;
+    const float* r;    /* r_k */
+    const float* T;    /* smoothing prefix table */
 } word_ctx;
+
+/* First k in [lo, hi) with x < T[k] (T non-decreasing, so a binary search), else -1. */
+static int32_t first_above(const float* T, int32_t lo, int32_t hi, float x) {
+    if (lo >= hi || !(x < T[hi - 1])) return -1;
+    while (lo < hi) {
+        const int32_t mid = lo + (hi - lo) / 2;
+        if (x < T[mid]) hi = mid; else lo = mid + 1;
+    }
+    return lo;
+}
+
+/* The Q-bucket draw of a split word for t = target - pS: the word's own topics first (rounds
+ * of 32 entries: carry + Kogge-Stone scan of alpha * (n_wk * r_k), the max topic's term 0;
+ * the first entry with a non-zero term whose prefix exceeds t, else the last such entry),
+ * then smoothing for t' = t - Qw against the table T with the max topic left out: the first
+ * k < maxK with t' < T[k] when t' < T[maxK-1], else the first k > maxK with
+ * t' + sm_max < T[k], else the last topic other than maxK. */
+static int32_t draw_q_split(const word_ctx* w, float t) {
+    if (t < w->Qw) {
+        float carry = 0.0f;
+        int32_t last = -1;
+        for (int32_t base = 0; base < w->nw; base += LANES) {
+            float tr[LANES], P[LANES];
+            for (int i = 0; i < LANES; ++i) {
+                const int32_t e = base + i;
+                tr[i] = (e < w->nw && w->wk[e] != w->maxK) ? w->alpha * ((float)w->wn[e] * w->r[w->wk[e]]) : 0.0f;
+            }
+            ks_scan32(tr, P);
+            for (int i = 0; i < LANES; ++i) P[i] = carry + P[i];
+            for (int i = 0; i < LANES && base + i < w->nw; ++i)
+                if (tr[i] > 0.0f && t < P[i]) return w->wk[base + i];
+            for (int i = 0; i < LANES && base + i < w->nw; ++i)
+                if (tr[i] > 0.0f) last = w->wk[base + i];
+            carry = P[LANES - 1];
+        }
+        if (last >= 0) return last;
+    }
+    const float t1 = t - w->Qw;
+    const int32_t m = w->maxK;
+    if (m > 0 && t1 < w->T[m - 1]) return first_above(w->T, 0, m, t1);
+    const float t2 = t1 + w->alpha * (w->beta * w->r[m]);
+    const int32_t k = first_above(w->T, m + 1, w->K, t2);
+    if (k >= 0) return k;
+    return m == w->K - 1 ? w->K - 2 : w->K - 1;
+}
 
 enum { BR_MAX = 0, BR_S = 1, BR_Q = 2 };
 
@@ -554,6 +674,7 @@ static int32_t draw_token(const word_ctx* w, const uint32_t* row, int32_t nnz, i
     }
     *branch = BR_Q;
     const float tt = target - pS;
+    if (w->split) return draw_q_split(w, tt);
     const int l = pick_lane(tt, w->QP, w->QL);
     const float t2 = tt - (l > 0 ? w->QP[l - 1] : 0.0f);
     if (l < 0) return w->maxK;
@@ -579,19 +700,48 @@ static int32_t draw_token(const word_ctx* w, const uint32_t* row, int32_t nnz, i
     return last >= 0 ? last : w->maxK;
 }
 
-/* Fills the word context of word w (its column with colz[maxK] = 0). */
-static void word_ctx_of(const orc_state* s, int32_t w, int32_t* cnt, float* colz, float* QP, word_ctx* wc) {
+/* Fills the word context of word w (its column with colz[maxK] = 0).  A split word gets
+ * its own topics and counts in wk / wn (K entries each).  With lane_q a split word instead
+ * draws its Q bucket by lane partials formed here from the column (the fold-in's
+ * specification, which has no sparse word rows), into ql. */
+static void word_ctx_of(const orc_state* s, int32_t w, int32_t* cnt, float* colz, float* QP, word_ctx* wc,
+                        int32_t* wk, int32_t* wn, float* ql, int lane_q) {
     word_column(s, w, cnt, colz);
     wc->K = s->K;
     wc->alpha = s->alpha;
+    wc->beta = s->beta;
     wc->maxK = (int32_t)(s->top2[w] & 0xffffu);
     wc->phi1 = s->phi4[(int64_t)w * 4 + 0];
     wc->phi2 = s->phi4[(int64_t)w * 4 + 1];
     wc->phi3 = s->phi4[(int64_t)w * 4 + 2];
+    wc->split = split_word(s, w) && !lane_q;
     wc->QL = s->ql + (int64_t)w * LANES;
+    if (split_word(s, w) && lane_q) {
+        for (int l = 0; l < LANES; ++l) {
+            float acc = 0.0f;
+            for (int32_t k = l; k < s->K; k += LANES)
+                if (k != wc->maxK) acc = fmaf(s->alpha, colz[k], acc);
+            ql[l] = acc;
+        }
+        wc->QL = ql;
+    }
     ks_scan32(wc->QL, QP);
     wc->QP = QP;
     wc->Q = QP[LANES - 1];
+    if (wc->split) {
+        wc->Qw = s->ql[(int64_t)w * LANES];
+        wc->Qs = s->ql[(int64_t)w * LANES + 1];
+        wc->Q = s->phi4[(int64_t)w * 4 + 3];
+        int32_t n = 0;
+        for (int32_t k = 0; k < s->K; ++k)
+            if (cnt[k]) { wk[n] = k; wn[n] = cnt[k]; ++n; }
+        wc->wk = wk;
+        wc->wn = wn;
+        wc->nw = n;
+        wc->r = s->r;
+        wc->T = s->T;
+        wc->Tsum = s->Tsum;
+    }
     colz[wc->maxK] = 0.0f;
     wc->colz = colz;
 }
@@ -608,7 +758,7 @@ static void sp_words(void* c, int64_t b, int64_t e, int tid) {
         if (s->woff[w + 1] == s->woff[w]) continue;
         float QP[LANES];
         word_ctx wc;
-        word_ctx_of(s, (int32_t)w, cnt, colz, QP, &wc);
+        word_ctx_of(s, (int32_t)w, cnt, colz, QP, &wc, cnt + s->K, cnt + 2 * (size_t)s->K, NULL, 0);
         double wll = 0.0;
         for (int64_t j = s->woff[w]; j < s->woff[w + 1]; ++j) {
             const int64_t t = s->wtok[j];
@@ -651,7 +801,7 @@ int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter, int3
     x.part = (orc_sample_stats*)calloc((size_t)nt, sizeof(orc_sample_stats));
     x.wll = (double*)calloc((size_t)s->V, sizeof(double));
     for (int t = 0; t < nt; ++t) {
-        x.icnt[t] = (int32_t*)calloc((size_t)s->K, sizeof(int32_t));
+        x.icnt[t] = (int32_t*)calloc((size_t)s->K * 3, sizeof(int32_t)); /* counts, split topics, split counts */
         x.fcol[t] = (float*)calloc((size_t)s->K, sizeof(float));
     }
     parallel_for(nt, s->V, 16, sp_words, &x);
@@ -723,7 +873,7 @@ int orc_foldin(const orc_state* s, const int32_t* words, int32_t len, uint32_t r
     const int32_t K = s->K;
     for (int32_t i = 0; i < len; ++i)
         if (words[i] < 0 || words[i] >= s->V) return -2;
-    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)K);
+    int32_t* cnt = (int32_t*)malloc(sizeof(int32_t) * (size_t)K * 3);
     int32_t* hist = (int32_t*)calloc((size_t)K, sizeof(int32_t));
     float* colz = (float*)malloc(sizeof(float) * (size_t)K);
     uint32_t* row = (uint32_t*)malloc(sizeof(uint32_t) * (size_t)K);
@@ -740,9 +890,9 @@ int orc_foldin(const orc_state* s, const int32_t* words, int32_t len, uint32_t r
         for (int32_t k = 0; k < K; ++k)
             if (hist[k]) row[nnz++] = ((uint32_t)k << 16) | (uint32_t)hist[k];
         for (int32_t i = 0; i < len; ++i) {
-            float QP[LANES];
+            float QP[LANES], qlf[LANES];
             word_ctx wc;
-            word_ctx_of(s, words[i], cnt, colz, QP, &wc);
+            word_ctx_of(s, words[i], cnt, colz, QP, &wc, cnt + K, cnt + 2 * (size_t)K, qlf, 1);
             const int32_t cmax = hist[wc.maxK];
             const int32_t c2 = hist[s->top2[words[i]] >> 16];
             const float u = orc_foldin_uniform(seed, rid, (uint32_t)sw, (uint32_t)i);

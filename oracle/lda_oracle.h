@@ -79,6 +79,11 @@ typedef struct {
 int orc_sample(orc_state* s, uint16_t* z_out, uint64_t seed, uint32_t iter,
                int32_t ll_mode, int32_t word_stride, orc_sample_stats* st);
 
+/* Words [0, Vd) are the trainer's dense words (default 0).  Above 2048 topics a sparse
+ * word (w >= Vd) splits its Q bucket into its own topics and a word-independent smoothing
+ * part; the rebuild's statistics and the draws follow.  Call before orc_rebuild. */
+int orc_set_num_dense(orc_state* s, int32_t Vd);
+
 /* Restricts orc_sample / orc_iterate to the tokens of docs [d0, d1) (the documents of a
  * range of chunks: what one rank of a document-sharded sweep samples); the others keep
  * their topics.  The default is every document. */

@@ -20,7 +20,8 @@ LL_RTOL = 1e-9
 def _setup(corpus, K, seed=42, nthreads=0):
     i = corpus.info
     tr = L.Trainer(corpus, K=K, seed=seed)
-    o = Oracle(corpus.tok_word(), corpus.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, nthreads=nthreads)
+    o = Oracle(corpus.tok_word(), corpus.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, nthreads=nthreads,
+               num_dense=i.num_dense)
     return tr, o
 
 
@@ -129,7 +130,7 @@ def test_large_k_dense_words_bit_exact(K, preset, alpha, stream_mode):
     assert i.num_dense > 0
     tr = L.Trainer(c, K=K, alpha=alpha, seed=11, stream_mode=stream_mode, num_streams=2)
     assert tr.stream_info()[0] is (stream_mode == 2)
-    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta)
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, num_dense=i.num_dense)
     z = c.topics()
     for it in range(3):
         ll = it != 1  # sweeps 0 and 2 run the LL-mode kernels, sweep 1 the plain ones
@@ -305,7 +306,7 @@ def test_config1_full_size_properties():
     tr.end_sweep()
     z1 = tr.topics()
     assert np.isfinite(ll) and z1.max() < K
-    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta)
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, num_dense=i.num_dense)
     o.rebuild(z0)
     zo = z0.copy()
     st = o.sample(zo, 42, 0, word_stride=97)
@@ -353,7 +354,8 @@ def test_streaming_by_budget_and_stage_api():
     stm = L.Trainer(c, K=K, seed=42, device_budget=full - 1, num_streams=2)
     assert stm.stream_info()[0]
     assert stm.device_bytes <= full - 1
-    o = Oracle(c.tok_word(), c.tok_doc(), c.info.vocab, c.info.num_docs, K, stm.alpha, stm.beta)
+    o = Oracle(c.tok_word(), c.tok_doc(), c.info.vocab, c.info.num_docs, K, stm.alpha, stm.beta,
+               num_dense=c.info.num_dense)
     z = c.topics()
     o.iterate(z, 42, 0)
     stm.update_wt()

@@ -20,7 +20,7 @@ def _trained(K, sweeps=5, preset="c0", **over):
     i = c.info
     tr = L.Trainer(c, K=K, seed=42)
     tr.iterate(sweeps)
-    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta)
+    o = Oracle(c.tok_word(), c.tok_doc(), i.vocab, i.num_docs, K, tr.alpha, tr.beta, num_dense=i.num_dense)
     o.rebuild(tr.topics())
     return c, tr, o
 
@@ -49,9 +49,11 @@ def test_model_phi_matches_oracle(K):
         assert np.array_equal(m.phi(w).view(np.uint32), o.phi_row(w).view(np.uint32)), f"word {w}"
 
 
-@pytest.mark.parametrize("K,item", [(16, 32), (64, 32), (1024, 32), (64, 256), (1024, 96)])
+@pytest.mark.parametrize("K,item", [(16, 32), (64, 32), (1024, 32), (64, 256), (1024, 96), (4096, 32)])
 def test_foldin_bit_exact(K, item):
-    """Work items of `item` tokens: a request spans up to 94 items on different warps."""
+    """Work items of `item` tokens: a request spans up to 94 items on different warps.
+    K=4096: the trainer's sparse words carry split Q statistics, which the model turns back
+    into lane partials from its phi rows (the fold-in's specification)."""
     c, tr, o = _trained(K)
     m = Model(tr)
     sweeps = 12

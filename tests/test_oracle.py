@@ -106,6 +106,43 @@ def test_sampler_distribution_matches_exact_conditional():
         assert draws[t][~m].sum() <= max(20, 3 * exp[~m].sum() + 10)
 
 
+def test_split_q_distribution_matches_exact_conditional():
+    """Above 2048 topics a sparse word draws its Q bucket in two parts (its own topics,
+    then the smoothing table).  Chi-square of the oracle's draws over sweep keys against the
+    FP64 conditional, with the high-mass topics as their own bins and the rest pooled in
+    blocks of 64 topics (alpha = 0.5 gives the Q bucket most of the mass)."""
+    K = 4096
+    c = L.Corpus.generate(L.corpus_config("c0", num_docs=30, vocab=50, K=K, num_chunks=1, corpus_seed=8,
+                                          len_p1=60.0))
+    i = c.info
+    assert i.num_dense == 0
+    tw, td, z = c.tok_word(), c.tok_doc(), c.topics()
+    o = Oracle(tw, td, i.vocab, i.num_docs, K, 0.5, 0.01, nthreads=4, num_dense=0)
+    o.rebuild(z)
+    q = o.word_stats()[3]
+    assert (q[:, 2:] == 0).all() and (q[:, 1] > 0).all()  # split statistics {Qw, Qs, 0, ...}
+    toks = [0, len(z) // 2, len(z) - 1]
+    n = 6000
+    draws = {t: np.zeros(K, np.int64) for t in toks}
+    zz = z.copy()
+    for it in range(n):
+        zz[:] = z
+        o.sample(zz, 77, it)
+        for t in toks:
+            draws[t][zz[t]] += 1
+    for t in toks:
+        p = o.token_probs(t)
+        exp = p * n
+        big = exp > 20
+        blk = np.arange(K) // 64
+        obs = np.concatenate([draws[t][big], np.bincount(blk[~big], draws[t][~big], minlength=64)])
+        ex = np.concatenate([exp[big], np.bincount(blk[~big], exp[~big], minlength=64)])
+        m = ex > 5
+        chi2 = (((obs - ex) ** 2)[m] / ex[m]).sum()
+        dof = m.sum() - 1
+        assert chi2 < dof + 4.5 * np.sqrt(2 * dof) + 10, (t, chi2, dof)
+
+
 def test_early_accept_is_exact_in_fp64():
     """A token settled by the max-topic bound gets maxK; in FP64 its u is below
     p_max / total, so the full evaluation would also pick maxK (EZLDA/utility.cu:1341-1373)."""
