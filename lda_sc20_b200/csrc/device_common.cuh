@@ -283,29 +283,28 @@ __host__ __device__ __forceinline__ int qtab_rounds(int K) {
     return (R >= 2 && R <= 16) ? R : 0;
 }
 
-// warp_level2_rounds (QB = 1 order) with the rounds' totals and largest lane prefixes known
-// (tab[r] = (KS total of round r, max over lanes of its KS prefix)).  Round r can hold the
-// crossing only if t2 < carry + max prefix; other rounds only add their total to the carry,
-// with the same additions in the same order, so the round that is evaluated sees the same
-// carry and gives the same topic.  Returns -1 when no evaluated round crosses; the caller
-// then runs the full search, which also finds the fallback topic.
+// warp_level2_rounds (QB = 1 order) with each round's carry and threshold known
+// (tab[r] = (carry before round r, carry + the round's largest KS lane prefix), the carry
+// being the fadd chain of the round totals).  Round r can hold the crossing only if
+// t2 < its threshold; one ballot over the R <= 32 rounds gives every such round, and they
+// are evaluated in order with the same carry the round-by-round walk reaches, so the
+// topic is the one warp_level2_rounds finds.  Returns -1 when no evaluated round crosses;
+// the caller then runs the full search, which also finds the fallback topic.
 template <class Slot>
 __device__ __forceinline__ int warp_level2_table(uint32_t n, float t2, int lane, Slot slot, const float2* tab) {
     const uint32_t R = (n + 31u) >> 5;
-    float carry = 0.0f;
-    for (uint32_t r = 0; r < R; ++r) {
-        const float2 tm = tab[r];
-        if (t2 < fadd(carry, tm.y)) {
-            int key = -1;
-            float ks = 0.0f;
-            bool ok = false;
-            const uint32_t i = 32u * r + lane;
-            if (i < n) slot(i, key, ks, ok);
-            ks = warp_ks_scan(ks, lane);
-            const unsigned f = __ballot_sync(FULL, ok && t2 < fadd(carry, ks));
-            if (f) return __shfl_sync(FULL, key, __ffs(f) - 1);
-        }
-        carry = fadd(carry, tm.x);
+    for (unsigned b = __ballot_sync(FULL, (uint32_t)lane < R && t2 < tab[lane < (int)R ? lane : 0].y); b;
+         b &= b - 1u) {
+        const uint32_t r = (uint32_t)(__ffs(b) - 1);
+        const float carry = tab[r].x;
+        int key = -1;
+        float ks = 0.0f;
+        bool ok = false;
+        const uint32_t i = 32u * r + lane;
+        if (i < n) slot(i, key, ks, ok);
+        ks = warp_ks_scan(ks, lane);
+        const unsigned f = __ballot_sync(FULL, ok && t2 < fadd(carry, ks));
+        if (f) return __shfl_sync(FULL, key, __ffs(f) - 1);
     }
     return -1;
 }
@@ -333,24 +332,22 @@ using ColShared = ColSharedT<false>;
 // entries (one fmaf chain).  A warp's loads of one step then read 32 consecutive entries,
 // one or two 128-byte lines, where contiguous per-lane blocks would touch one line per
 // lane block.
-#ifndef LDA_ROW_MODE
-#define LDA_ROW_MODE 0
-#endif
-template <class View>
+// ROWM 1: the loads of four steps, then of two, then one, are issued before their use
+// (rows that often miss L2, at large K); ROWM 0: two steps at a time.
+template <int ROWM = 0, class View>
 __device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uint32_t lane, uint32_t nnz,
                                            const View& colz, float acc = 0.0f) {
     uint32_t q = lane;
-#if LDA_ROW_MODE == 1
-    // the loads of four steps, then of two, then one, issued before their use
-    for (; q + 96u < nnz; q += 128u) {
+    if (ROWM == 1) {
+        for (; q + 96u < nnz; q += 128u) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
                        e3 = __ldg(row + q + 96u);
         acc = ffma(u2f(e0 & 0xffffu), colz.row(e0 >> 16), acc);
         acc = ffma(u2f(e1 & 0xffffu), colz.row(e1 >> 16), acc);
         acc = ffma(u2f(e2 & 0xffffu), colz.row(e2 >> 16), acc);
         acc = ffma(u2f(e3 & 0xffffu), colz.row(e3 >> 16), acc);
+        }
     }
-#endif
     // the loads of two steps issued together
     for (; q + 32u < nnz; q += 64u) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);

@@ -421,7 +421,7 @@ enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 // The 32-token groups g0, g0 + gstep, ... of the token range [start, start + cnt) of one
 // word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word).
 // Returns the lane's LL partial (LL mode).
-template <bool LL, int QB, bool SPLIT = false, class View>
+template <bool LL, int QB, bool SPLIT = false, int ROWM = 0, class View>
 __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t start, uint32_t cnt, uint32_t g0,
                                                 uint32_t gstep, uint32_t iter, int maxK, const float4 ph, float QL,
                                                 float QP, float Q, const View& colz, uint32_t* ctr, int lane,
@@ -500,7 +500,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 float acc = 0.0f;
                 if ((uint32_t)lane < nnz) acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
                 if ((uint32_t)lane + 32u < nnz) acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
-                SL = lane_mass(row, (uint32_t)lane + 64u, nnz, colz, acc);
+                SL = lane_mass<ROWM>(row, (uint32_t)lane + 64u, nnz, colz, acc);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
             }
@@ -510,7 +510,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 cur = dj;
                 nnz = __shfl_sync(FULL, my_nnz, j);
                 row = a.dt_ent + __shfl_sync(FULL, my_off, j);
-                SL = lane_mass(row, (uint32_t)lane, nnz, colz);
+                SL = lane_mass<ROWM>(row, (uint32_t)lane, nnz, colz);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
                 evaluated |= (lane == j);
