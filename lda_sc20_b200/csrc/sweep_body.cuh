@@ -394,6 +394,9 @@ enum { C_TOK, C_EA, C_FULL, C_NNZ, C_MAX, C_S, C_Q, C_WNNZ, C_TDENSE, C_TSPARSE,
 // per SM it is compiled for: the register cap is 65536 / (32 * warps * blocks) per
 // thread.  The LL-mode kernel (its FP64 term) and the K > 1024 kernel (four Q rounds per
 // batch) keep more state live and are compiled for fewer.
+// Branch taken by a token (counters only).
+enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
+
 #ifndef LDA_SAMPLE_WARPS
 #define LDA_SAMPLE_WARPS 8
 #endif
@@ -410,13 +413,6 @@ constexpr int kSampleWarps = LDA_SAMPLE_WARPS;
 #ifndef LDA_SPARSE_LARGE_MIN_BLOCKS
 #define LDA_SPARSE_LARGE_MIN_BLOCKS 4
 #endif
-
-#ifndef LDA_ROW_PREFETCH
-#define LDA_ROW_PREFETCH 0
-#endif
-
-// Branch taken by a token (counters only).
-enum { BR_NONE = 0, BR_MAX = 1, BR_S = 2, BR_Q = 3 };
 
 // The 32-token groups g0, g0 + gstep, ... of the token range [start, start + cnt) of one
 // word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word).
@@ -435,6 +431,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
     uint32_t cur = 0xffffffffu, nnz = 0;
     const uint32_t* row = a.dt_ent;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
+    unsigned spos = 0u;  // lanes of the current row with a positive sum
     for (uint32_t g = g0; g < cnt; g += gstep) {
         const bool valid = g + lane < cnt;
         const uint32_t tok = start + g + lane;
@@ -456,8 +453,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
         }
         int znew = maxK;
         // per-lane record of this token's evaluation, for the deferred draw and counters
-        const uint32_t* my_row = row;
-        uint32_t my_ls = 0, my_nnz_s = 0;
+        uint32_t my_ls = 0;
         float my_t2 = 0.0f, my_total = 0.0f;
         int kind = BR_NONE;
         bool evaluated = false;
@@ -465,46 +461,9 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
         const unsigned emask = __ballot_sync(FULL, ea);
         const unsigned need0 = LL ? vmask : (vmask & ~emask);
         unsigned need = need0;
-#if LDA_ROW_PREFETCH
-        // the needed tokens that start a new row: the first whose doc differs from `cur`,
-        // then each whose doc differs from the previous needed token's
-        const unsigned below = need0 & ((1u << lane) - 1u);
-        const uint32_t dprev = __shfl_sync(FULL, d, below ? 31 - __clz(below) : lane);
-        const bool newrow = ((need0 >> lane) & 1u) && d != (below ? dprev : cur);
-        unsigned rows = __ballot_sync(FULL, newrow);
-        evaluated = newrow;
-        if (need0) cur = __shfl_sync(FULL, d, 31 - __clz(need0));
-        // the first two steps of the next row to evaluate are loaded one row ahead
-        uint32_t pf_nnz = 0, pf_off = 0, pf0 = 0, pf1 = 0;
-        auto prefetch = [&](unsigned rest) {
-            if (rest) {
-                const int j2 = __ffs(rest) - 1;
-                pf_nnz = __shfl_sync(FULL, my_nnz, j2);
-                pf_off = __shfl_sync(FULL, my_off, j2);
-                const uint32_t* r2 = a.dt_ent + pf_off;
-                pf0 = (uint32_t)lane < pf_nnz ? __ldg(r2 + lane) : 0u;
-                pf1 = (uint32_t)lane + 32u < pf_nnz ? __ldg(r2 + lane + 32) : 0u;
-            }
-        };
-        prefetch(rows);
-#endif
         while (need) {
             const int j = __ffs(need) - 1;
             need &= need - 1u;
-#if LDA_ROW_PREFETCH
-            if ((rows >> j) & 1u) {
-                nnz = pf_nnz;
-                row = a.dt_ent + pf_off;
-                const uint32_t e0 = pf0, e1 = pf1;
-                prefetch(j == 31 ? 0u : rows & (0xfffffffeu << j));
-                float acc = 0.0f;
-                if ((uint32_t)lane < nnz) acc = ffma(u2f(e0 & 0xffffu), colz((int)(e0 >> 16)), acc);
-                if ((uint32_t)lane + 32u < nnz) acc = ffma(u2f(e1 & 0xffffu), colz((int)(e1 >> 16)), acc);
-                SL = lane_mass<ROWM>(row, (uint32_t)lane + 64u, nnz, colz, acc);
-                SP = warp_ks_scan(SL, lane);
-                S = __shfl_sync(FULL, SP, 31);
-            }
-#else
             const uint32_t dj = __shfl_sync(FULL, d, j);
             if (dj != cur) {
                 cur = dj;
@@ -513,9 +472,9 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 SL = lane_mass<ROWM>(row, (uint32_t)lane, nnz, colz);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
+                spos = __ballot_sync(FULL, SL > 0.0f);
                 evaluated |= (lane == j);
             }
-#endif
             const float pmj = __shfl_sync(FULL, pmax, j);
             const float uj = __shfl_sync(FULL, u, j);
             const float pS = fadd(pmj, S);
@@ -528,14 +487,11 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
             } else if (target < pS) {
                 const float tt = fsub(target, pmj);
                 const unsigned cand = __ballot_sync(FULL, tt < SP && SL > 0.0f);
-                const unsigned pos = __ballot_sync(FULL, SL > 0.0f);
-                const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(pos);
+                const int ls = cand ? __ffs(cand) - 1 : 31 - __clz(spos);
                 const float prev = __shfl_sync(FULL, SP, ls > 0 ? ls - 1 : 0);
                 if (lane == j) {
                     kind = BR_S;
-                    my_row = row;
                     my_ls = (uint32_t)ls;
-                    my_nnz_s = nnz;
                     my_t2 = ls > 0 ? fsub(tt, prev) : tt;
                 }
             } else {
@@ -579,7 +535,8 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
                 ll_n = 0;
             }
         }
-        if (kind == BR_S) znew = lane_draw(my_row, my_ls, my_nnz_s, colz, my_t2, maxK);
+        // an S-bucket token's row is its own doc's: the lane holds its offset and length
+        if (kind == BR_S) znew = lane_draw(a.dt_ent + my_off, my_ls, my_nnz, colz, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
         const bool in_need = (need0 >> lane) & 1u;
