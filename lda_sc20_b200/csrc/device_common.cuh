@@ -325,6 +325,9 @@ struct ColSharedT {
     __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
     __device__ __forceinline__ float row(uint32_t key) const { return col[SKEWKEYS ? (int)key : col_skew((int)key)]; }
     __device__ __forceinline__ int topic(uint32_t key) const { return SKEWKEYS ? col_unskew((int)key) : (int)key; }
+    // an entry is (key << 16) | count
+    __device__ __forceinline__ uint32_t key(uint32_t e) const { return e >> 16; }
+    __device__ __forceinline__ float cnt(uint32_t e) const { return u2f(e & 0xffffu); }
 };
 using ColShared = ColSharedT<false>;
 
@@ -342,21 +345,21 @@ __device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uin
         for (; q + 96u < nnz; q += 128u) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
                        e3 = __ldg(row + q + 96u);
-        acc = ffma(u2f(e0 & 0xffffu), colz.row(e0 >> 16), acc);
-        acc = ffma(u2f(e1 & 0xffffu), colz.row(e1 >> 16), acc);
-        acc = ffma(u2f(e2 & 0xffffu), colz.row(e2 >> 16), acc);
-        acc = ffma(u2f(e3 & 0xffffu), colz.row(e3 >> 16), acc);
+        acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
+        acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
+        acc = ffma(colz.cnt(e2), colz.row(colz.key(e2)), acc);
+        acc = ffma(colz.cnt(e3), colz.row(colz.key(e3)), acc);
         }
     }
     // the loads of two steps issued together
     for (; q + 32u < nnz; q += 64u) {
         const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
-        acc = ffma(u2f(e0 & 0xffffu), colz.row(e0 >> 16), acc);
-        acc = ffma(u2f(e1 & 0xffffu), colz.row(e1 >> 16), acc);
+        acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
+        acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
     }
     if (q < nnz) {
         const uint32_t e = __ldg(row + q);
-        acc = ffma(u2f(e & 0xffffu), colz.row(e >> 16), acc);
+        acc = ffma(colz.cnt(e), colz.row(colz.key(e)), acc);
     }
     return acc;
 }
@@ -378,9 +381,9 @@ __device__ __forceinline__ int lane_draw(const uint32_t* __restrict__ row, uint3
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             if (q + 32u * s >= nnz) break;
-            const uint32_t key = e[s] >> 16;
+            const uint32_t key = colz.key(e[s]);
             const float cz = colz.row(key);
-            acc = ffma(u2f(e[s] & 0xffffu), cz, acc);
+            acc = ffma(colz.cnt(e[s]), cz, acc);
             if (cz > 0.0f) {
                 last = (int)key;
                 if (t2 < acc) return colz.topic(key);

@@ -129,6 +129,8 @@ struct ColBits {
     }
     __device__ __forceinline__ float row(uint32_t key) const { return (*this)((int)key); }
     __device__ __forceinline__ int topic(uint32_t key) const { return (int)key; }
+    __device__ __forceinline__ uint32_t key(uint32_t e) const { return e >> 16; }
+    __device__ __forceinline__ float cnt(uint32_t e) const { return u2f(e & 0xffffu); }
 };
 
 __host__ __device__ __forceinline__ int large_bit_words(int K) { return (K + 31) >> 5; }
