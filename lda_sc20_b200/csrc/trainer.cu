@@ -35,7 +35,10 @@ constexpr int kSampleTileMin = 64;            // fewest tokens per tile that a c
 // A chunk's sampler tiles are sized so that each resident warp gets about this many:
 // with fewer, the launch ends with the longest tile while most warps sit idle.
 constexpr int kTilesPerWarp = LDA_TILES_PER_WARP;
-constexpr int kDenseTileLarge = 2048;         // dense-word tiles above kLargeK topics (one CTA per tile)
+#ifndef LDA_DENSE_TILE
+#define LDA_DENSE_TILE 8192
+#endif
+constexpr int kDenseTileLarge = LDA_DENSE_TILE;  // dense-word tiles above kLargeK topics (one CTA per tile)
 constexpr int kLargeWarps = 8;                // warps per CTA of the large-K sampler kernels
 constexpr int kWtTile = 16384;     // tokens per dense word-topic tile
 constexpr int kCounters = 16;
@@ -1417,8 +1420,9 @@ extern "C" int lda_get_token_meta(lda_trainer* t, uint32_t* meta) {
 // lda_sample_chunk_noalloc runs the same k_sample / k_ll_reduce kernels on buffers the
 // caller owns.  Its scratch lives in one file-scope device array: bytes [0,4) the tile
 // counter, [8,136) the sweep counters, [256, 256 + 8*kNoAllocMaxTiles) the per-tile LL
-// partials, then (K > 2048) the smoothing table of the split Q bucket, K floats.  In host code the symbol is only a host-side stand-in, so the device address
-// is looked up once per device (with that device current) and cached.
+// partials, then (K > 2048) the smoothing table of the split Q bucket, K floats.  In host
+// code the symbol is only a host-side stand-in, so the device address is looked up once
+// per device (with that device current) and cached.
 
 namespace {
 constexpr int kNoAllocMaxTiles = 65536;
