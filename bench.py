@@ -207,9 +207,9 @@ def sampler_algorithmic_bytes(cnt, K: int, dense_words_per_sweep: int, sweeps: i
 
 
 def run_sharded(args, world, rank, local):
-    """N GPUs, one process each: the corpus is split by chunks (documents) and the ranks
-    exchange their chunks' topics after every sweep (lda_sc20_b200.sharded).  Total work
-    is fixed, so this is strong scaling."""
+    """N GPUs, one process each: the corpus is split by chunks (documents) for sampling and
+    by word ranges for the word side, and the ranks exchange both every sweep
+    (lda_sc20_b200.sharded).  Total work is fixed, so this is strong scaling."""
     import datetime
     import numpy as np
     import torch
@@ -275,7 +275,7 @@ def run_sharded(args, world, rank, local):
         for _ in range(args.steps):
             st.z[a:b].copy_(hin, non_blocking=True)
             st.ex.exchange()
-            st.tr.iterate(1)
+            st.sweep()
             hout.copy_(st.z[a:b])
             hin, hout = hout, hin
         torch.cuda.synchronize()
@@ -297,7 +297,9 @@ def run_sharded(args, world, rank, local):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(args.preset, args.chunks), "tokens_per_step": N, "dense_words": info.num_dense,
-            "run": {"parallelism": f"doc-sharded x{world}: chunks {st.ranges}, NCCL topic exchange per sweep"},
+            "run": {"parallelism": f"doc-sharded x{world}: chunks {st.ranges}, word ranges {st.word_ranges}; "
+                                       "per sweep an n_k all-reduce, a word-side all-gather "
+                                       f"({st.wx.bytes_per_rank} B per rank) and a topic all-gather"},
             "loglik_per_token": ll_mean, "ranks_agree": agree, "e2e": e2e,
             "gpu_launches": tm.launches_wt + tm.launches_stats + tm.launches_dt + tm.launches_sample + tm.launches_ll,
             "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak, "unit": "GB/s",

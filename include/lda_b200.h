@@ -184,6 +184,37 @@ int lda_trainer_set_chunk_range(lda_trainer* t, int32_t first, int32_t last);
 /* Device address and length of the trainer's topic array (uint16, word-sorted), for a
  * collective that exchanges topic slices in place between sweeps. */
 int lda_trainer_topics_device(lda_trainer* t, void** ptr, int64_t* count);
+/* Restricts lda_update_wt and lda_max_topic to the words [w0, w1) (default: all): the
+ * rebuild zeroes and refills only the range's dense rows and sparse rows, and n_k receives
+ * only the range's tokens; the statistics are computed for the range's words only.  A
+ * word-sharded run gives each rank a disjoint range, sums n_k over the ranks before
+ * lda_max_topic, gathers every range's rows and statistics afterwards, and then calls
+ * lda_trainer_sweep_chunks.  Replaces the replicated UpdateWT / MaxTopic pass that every
+ * GPU of a multi-GPU form would otherwise run (EZLDA/mainKernel.cu:282-290). */
+int lda_trainer_set_word_range(lda_trainer* t, int32_t w0, int32_t w1);
+/* Device addresses of the word side a word-sharded run exchanges.  Words [0, num_dense)
+ * have dense rows (dense_wt, K int32 each); word num_dense + s has the sparse row
+ * sparse_ent[sparse_off[s] .. sparse_off[s] + sparse_nnz[s]) inside a fixed slot that ends
+ * at sparse_off[s + 1] (sparse_capacity for the last word).  Per word: top2 and k3
+ * (uint32), phi4 (4 floats), ql (32 floats). */
+typedef struct lda_word_side {
+    int32_t* n_k;
+    int32_t* dense_wt;
+    uint32_t* sparse_ent;
+    uint32_t* sparse_nnz;
+    const uint32_t* sparse_off;
+    uint32_t* top2;
+    uint32_t* k3;
+    float* phi4;
+    float* ql;
+    int64_t K, vocab, num_dense, sparse_capacity;
+} lda_word_side;
+int lda_trainer_word_side(lda_trainer* t, lda_word_side* out);
+/* One sweep without its word side: the caller has run lda_update_wt and lda_max_topic (and
+ * exchanged their results) for this sweep's starting topics.  Runs the chunk range's
+ * doc-topic rebuilds and sampling, the LL when ll_mode is set, and advances the
+ * iteration; returns when the sweep is done. */
+int lda_trainer_sweep_chunks(lda_trainer* t, int32_t ll_mode);
 
 /* n full sweeps of the driver loop EZLDA/mainKernel.cu:158-380 on resident
  * data; ll_mode=1 also evaluates the FP64 log-likelihood of every sweep.

@@ -15,7 +15,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import (CorpusInfo, GenConfig, LdaError, SweepCounters, StageTiming, TrainConfig,
+from ._native import (CorpusInfo, GenConfig, LdaError, SweepCounters, StageTiming, TrainConfig, WordSide,
                       check, load)
 
 __all__ = ["Corpus", "Trainer", "GenConfig", "LdaError", "corpus_config", "load"]
@@ -305,6 +305,21 @@ class Trainer:
     def set_chunk_range(self, first: int, last: int) -> None:
         """Sample (and rebuild doc rows for) chunks [first, last) only."""
         check(self._lib.lda_trainer_set_chunk_range(self._h, first, last))
+
+    def set_word_range(self, w0: int, w1: int) -> None:
+        """Rebuild word-topic rows and word statistics for words [w0, w1) only."""
+        check(self._lib.lda_trainer_set_word_range(self._h, w0, w1))
+
+    def word_side(self) -> _native.WordSide:
+        """Device addresses of n_k, the word-topic rows and the word statistics."""
+        ws = WordSide()
+        check(self._lib.lda_trainer_word_side(self._h, C.byref(ws)))
+        return ws
+
+    def sweep_chunks(self, ll: bool = False) -> None:
+        """One sweep whose word side (update_wt, max_topic) the caller has already made
+        current: the chunk range's doc-row rebuilds and sampling, then the LL."""
+        check(self._lib.lda_trainer_sweep_chunks(self._h, 1 if ll else 0))
 
     def topics_device(self) -> tuple[int, int]:
         """(device address, length) of the uint16 topic array."""

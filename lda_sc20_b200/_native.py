@@ -82,6 +82,15 @@ class SampleIO(C.Structure):
     ]
 
 
+class WordSide(C.Structure):
+    """lda_word_side: device addresses of a trainer's word side."""
+    _fields_ = [
+        ("n_k", C.c_void_p), ("dense_wt", C.c_void_p), ("sparse_ent", C.c_void_p), ("sparse_nnz", C.c_void_p),
+        ("sparse_off", C.c_void_p), ("top2", C.c_void_p), ("k3", C.c_void_p), ("phi4", C.c_void_p), ("ql", C.c_void_p),
+        ("K", C.c_int64), ("vocab", C.c_int64), ("num_dense", C.c_int64), ("sparse_capacity", C.c_int64),
+    ]
+
+
 P = C.c_void_p
 I32, I64, U32, U64, F32, F64 = C.c_int32, C.c_int64, C.c_uint32, C.c_uint64, C.c_float, C.c_double
 
@@ -104,6 +113,9 @@ SIGNATURES = {
     "lda_trainer_device_bytes": (I32, [P, C.POINTER(I64)]),
     "lda_trainer_set_chunk_range": (I32, [P, I32, I32]),
     "lda_trainer_topics_device": (I32, [P, C.POINTER(P), C.POINTER(I64)]),
+    "lda_trainer_set_word_range": (I32, [P, I32, I32]),
+    "lda_trainer_word_side": (I32, [P, C.POINTER(WordSide)]),
+    "lda_trainer_sweep_chunks": (I32, [P, I32]),
     "lda_trainer_iterate": (I32, [P, I32, I32]),
     "lda_iterate_host": (I32, [P, P, P, I32, C.POINTER(F64)]),
     "lda_iterate_host_async": (I32, [P, P, P]),

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
     float* col = smf + (size_t)a.K * (1 + wid);
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     __syncthreads();
-    for (int w = blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
+    for (int w = a.wlo + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
         word_stats_word(a, w, r, col, lane);
     }
 }
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
         pk = order[n];
         pv = fmul(a.beta, r[pk]);
     }
-    for (int w = a.Vd + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
+    for (int w = max(a.Vd, a.wlo) + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
         const int s = w - a.Vd;
         const uint32_t* ent = a.swt_ent + __ldg(a.swt_off + s);
         const uint32_t nnz = __ldg(a.swt_nnz + s);

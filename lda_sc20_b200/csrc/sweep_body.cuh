@@ -133,6 +133,7 @@ struct StatsArgs {
     float4* st_phi;     // {phi_max, phi_2nd, phi_3rd, Q}
     float* st_ql;       // [V*32]
     const float* smooth = nullptr;  // K > kLargeK: the smoothing table (k_smooth_table)
+    int wlo = 0;                    // the words [wlo, V) get statistics (a word range)
 };
 
 // Statistics of word w from its column (built into the warp's shared `col`).

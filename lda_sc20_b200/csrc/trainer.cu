@@ -107,6 +107,10 @@ struct lda_trainer {
     std::vector<bool> chunk_sampled_ll;
     int chunk_first = 0, chunk_last = 0;  // sampled chunk range of lda_trainer_iterate
     std::vector<int4> h_stiles, h_wtiles;  // host copies of the tile lists
+    // word range of the word-topic rebuild (lda_trainer_set_word_range): its tiles
+    int32_t wt_lo = 0, wt_hi = 0;
+    int4* w_tiles_rng = nullptr;
+    int n_wtiles_rng = 0;
 
     // streaming: the per-token arrays of the doc-topic rebuild and the sampler (doc of each
     // token, doc-order -> word-sorted map and word, per-token metadata) and the doc rows
@@ -180,6 +184,7 @@ struct lda_trainer {
         cudaFreeHost(h_dtok_pos);
         cudaFreeHost(h_dtok_word);
         for (void* p : allocs) cudaFree(p);
+        if (w_tiles_rng) cudaFree(w_tiles_rng);
         if (ll_host) cudaFreeHost(ll_host);
         for (auto& e : pending) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
         for (auto& e : pool) { cudaEventDestroy(e.a); cudaEventDestroy(e.b); }
@@ -631,6 +636,47 @@ extern "C" int lda_trainer_set_chunk_range(lda_trainer* t, int32_t first, int32_
     return LDA_OK;
 }
 
+extern "C" int lda_trainer_set_word_range(lda_trainer* t, int32_t w0, int32_t w1) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    if (w0 < 0 || w1 > t->V || w0 > w1) return fail(LDA_ERR_ARG, "word range [%d, %d) outside [0, %lld)", w0, w1, (long long)t->V);
+    CUDA_TRY(cudaSetDevice(t->device));
+    CUDA_TRY(cudaStreamSynchronize(t->stream));
+    if (t->w_tiles_rng) {
+        CUDA_TRY(cudaFree(t->w_tiles_rng));
+        t->w_tiles_rng = nullptr;
+        t->n_wtiles_rng = 0;
+    }
+    t->wt_lo = w0;
+    t->wt_hi = w1;
+    if (w0 == 0 && w1 == t->V) return LDA_OK;  // the whole vocabulary: the trainer's own tiles
+    // the range's tiles, in the trainer's largest-first order
+    std::vector<int4> r;
+    for (const int4& x : t->h_wtiles)
+        if (x.x >= w0 && x.x < w1) r.push_back(x);
+    CUDA_TRY(cudaMalloc(&t->w_tiles_rng, sizeof(int4) * std::max<size_t>(r.size(), 1)));
+    if (!r.empty()) CUDA_TRY(cudaMemcpy(t->w_tiles_rng, r.data(), sizeof(int4) * r.size(), cudaMemcpyHostToDevice));
+    t->n_wtiles_rng = (int)r.size();
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_word_side(lda_trainer* t, lda_word_side* out) {
+    if (!t || !out) return fail(LDA_ERR_ARG, "null argument");
+    out->n_k = t->n_k;
+    out->dense_wt = t->dwt;
+    out->sparse_ent = t->swt_ent;
+    out->sparse_nnz = t->swt_nnz;
+    out->sparse_off = t->swt_off;
+    out->top2 = t->st_top2;
+    out->k3 = t->st_k3;
+    out->phi4 = reinterpret_cast<float*>(t->st_phi);
+    out->ql = t->st_ql;
+    out->K = t->K;
+    out->vocab = t->V;
+    out->num_dense = t->Vd;
+    out->sparse_capacity = t->swt_cap;
+    return LDA_OK;
+}
+
 extern "C" int lda_trainer_topics_device(lda_trainer* t, void** ptr, int64_t* count) {
     if (!t || !ptr) return fail(LDA_ERR_ARG, "null argument");
     *ptr = (void*)t->z;
@@ -679,10 +725,19 @@ extern "C" int lda_update_wt(lda_trainer* t) {
     CUDA_TRY(cudaSetDevice(t->device));
     t->begin_stage(0);
     CUDA_TRY(cudaMemsetAsync(t->n_k, 0, sizeof(int) * (size_t)t->K, t->stream));
-    if (t->Vd > 0) CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
+    dev::WtArgs a = wt_args(t);
+    if (t->w_tiles_rng) {
+        // a word range: its dense rows, its sparse rows and its words' share of n_k
+        const int64_t d0 = std::min<int64_t>(t->wt_lo, t->Vd), d1 = std::min<int64_t>(t->wt_hi, t->Vd);
+        if (d1 > d0)
+            CUDA_TRY(cudaMemsetAsync(t->dwt + d0 * t->K, 0, sizeof(int) * (size_t)(d1 - d0) * t->K, t->stream));
+        a.tiles = t->w_tiles_rng;
+        a.ntiles = t->n_wtiles_rng;
+    } else if (t->Vd > 0) {
+        CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
+    }
     CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
-    const dev::WtArgs a = wt_args(t);
-    const int grid = std::max(1, std::min(t->grid_wt, (t->n_wtiles + t->warps_wt - 1) / t->warps_wt));
+    const int grid = std::max(1, std::min(t->grid_wt, (a.ntiles + t->warps_wt - 1) / t->warps_wt));
     dev::k_wt_build<true><<<grid, 32 * t->warps_wt, t->smem_wt, t->stream>>>(a);
     CUDA_TRY(cudaGetLastError());
     t->end_stage();
@@ -693,24 +748,32 @@ extern "C" int lda_max_topic(lda_trainer* t) {
     if (!t) return fail(LDA_ERR_ARG, "null trainer");
     CUDA_TRY(cudaSetDevice(t->device));
     t->begin_stage(1);
-    const dev::StatsArgs a = stats_args(t);
+    dev::StatsArgs a = stats_args(t);
+    if (t->w_tiles_rng) {
+        // a word range: its words' statistics only
+        a.wlo = t->wt_lo;
+        a.V = t->wt_hi;
+    }
     if (!t->large) {
-        dev::k_word_stats<<<t->grid_stats, 32 * t->warps, t->smem_stats, t->stream>>>(a);
-        CUDA_TRY(cudaGetLastError());
+        if (a.V > a.wlo) {
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats, (a.V - a.wlo + t->warps - 1) / t->warps));
+            dev::k_word_stats<<<grid, 32 * t->warps, t->smem_stats, t->stream>>>(a);
+            CUDA_TRY(cudaGetLastError());
+        }
     } else {
         // the smoothing table of the sparse words' split Q bucket, then dense words from
         // their columns, sparse words without one
         dev::k_smooth_table<<<1, 32, 0, t->stream>>>(t->n_k, t->K, t->Vbeta, t->alpha, t->beta, t->smooth);
         CUDA_TRY(cudaGetLastError());
-        if (t->Vd > 0) {
-            dev::StatsArgs ad = a;
-            ad.V = t->Vd;
-            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats, (t->Vd + t->warps - 1) / t->warps));
+        dev::StatsArgs ad = a;
+        ad.V = std::min(a.V, t->Vd);
+        if (ad.V > ad.wlo) {
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats, (ad.V - ad.wlo + t->warps - 1) / t->warps));
             dev::k_word_stats<<<grid, 32 * t->warps, t->smem_stats, t->stream>>>(ad);
             CUDA_TRY(cudaGetLastError());
         }
-        if (t->V > t->Vd) {
-            const int64_t ns = t->V - t->Vd;
+        if (a.V > std::max(t->Vd, a.wlo)) {
+            const int64_t ns = a.V - std::max(t->Vd, a.wlo);
             const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats_sparse, (ns + kLargeWarps - 1) / kLargeWarps));
             dev::k_word_stats_sparse_large<<<grid, 32 * kLargeWarps, t->smem_stats_sparse, t->stream>>>(a);
             CUDA_TRY(cudaGetLastError());
@@ -936,10 +999,16 @@ static int copy_back(lda_trainer* t, int ch, cudaStream_t q, uint16_t* zout) {
     return LDA_OK;
 }
 
-static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr) {
+// One sweep: the word side (rebuild + statistics) unless the caller has made it current,
+// then the chunk range's doc-row rebuilds and sampling, and the sweep's LL.
+static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bool word_side_done = false) {
     int rc;
-    if ((rc = lda_update_wt(t))) return rc;
-    if ((rc = lda_max_topic(t))) return rc;
+    if (!word_side_done) {
+        if (t->w_tiles_rng)
+            return fail(LDA_ERR_STATE, "a word range is set: the caller completes the word side and calls lda_trainer_sweep_chunks");
+        if ((rc = lda_update_wt(t))) return rc;
+        if ((rc = lda_max_topic(t))) return rc;
+    }
     if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2)) {
         // one stream, so that the stage events time each stage alone
         for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
@@ -1010,6 +1079,20 @@ extern "C" int lda_trainer_iterate(lda_trainer* t, int32_t n, int32_t ll_mode) {
     int rc = finish(t);
     if (rc) return rc;
     if (ll_mode && n > 0) {
+        t->last_ll = *t->ll_host;
+        t->last_ll_tokens = t->range_tokens();
+        t->ll_valid = true;
+    }
+    return LDA_OK;
+}
+
+extern "C" int lda_trainer_sweep_chunks(lda_trainer* t, int32_t ll_mode) {
+    if (!t) return fail(LDA_ERR_ARG, "null trainer");
+    CUDA_TRY(cudaSetDevice(t->device));
+    int rc = sweep_async(t, ll_mode, nullptr, true);
+    if (rc) return rc;
+    if ((rc = finish(t))) return rc;
+    if (ll_mode) {
         t->last_ll = *t->ll_host;
         t->last_ll_tokens = t->range_tokens();
         t->ll_valid = true;
