@@ -43,6 +43,286 @@ __global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
     }
 }
 
+// ---------------------------------------------------------------- large-K rebuilds
+// Above kLargeK topics a warp-private K-sized histogram leaves one 8-warp CTA per SM, and
+// the rebuilds wait on their gathers with little else to run (halving the histogram's
+// size to 16-bit counts halved both rebuilds' time).  These kernels share one histogram
+// across the CTA's 256 threads and take one unit at a time (a word tile, a doc), so that
+// eight CTAs per SM keep 64 warps of gathers in flight.  Their rows, counts, metadata and
+// errors are those of k_wt_build / k_dt_build, bit for bit; the topic totals come from
+// k_topic_totals.
+constexpr int kRebuildThreads = 256;
+
+// Exclusive scan of one value per thread across the CTA; *total gets the sum.  wsum holds
+// a word per warp.  Every thread of the CTA calls it.
+__device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t* wsum, uint32_t* total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t t = __shfl_up_sync(FULL, incl, off);
+        if (lane >= off) incl += t;
+    }
+    if (lane == 31) wsum[wid] = incl;
+    __syncthreads();
+    uint32_t before = 0, tot = 0;
+    for (int i = 0; i < nw; ++i) {
+        const uint32_t x = wsum[i];
+        before += i < wid ? x : 0u;
+        tot += x;
+    }
+    *total = tot;
+    __syncthreads();
+    return before + incl - v;
+}
+
+// Adds topics topic_of(i), i in [0, n), to the CTA's histogram (16-bit counts) and sets
+// the bit of each topic whose count leaves zero; a topic >= K sets *err and is skipped.
+// Four 256-token steps of loads are in flight per thread.  n is uniform across the CTA.
+template <class F>
+__device__ __forceinline__ void cta_hist(uint32_t n, const F& topic_of, const Hist<true>& hist, uint32_t* bits, int K,
+                                         int* err) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = 0; base < n; base += 4u * kRebuildThreads) {
+        uint32_t k[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            const uint32_t i = base + (uint32_t)(s * kRebuildThreads) + threadIdx.x;
+            k[s] = i < n ? topic_of(i) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+            if (base + (uint32_t)(s * kRebuildThreads) >= n) break;
+            bool valid = k[s] != 0xffffffffu;
+            uint32_t kk = k[s];
+            if (valid && kk >= (uint32_t)K) {
+                atomicOr(err, 1);
+                valid = false;
+                kk = 0xfffffffeu;
+            }
+            const unsigned m = __match_any_sync(FULL, kk);
+            if (valid && lane == __ffs(m) - 1) {
+                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
+            }
+        }
+    }
+}
+
+// Walks the CTA's bitmap (bw words) in ascending topic order: thread t takes words
+// [t R, t R + R), R = ceil(bw / threads), an exclusive scan of their popcounts places
+// its entries, and emit(k, count, position) is called for each non-zero topic; bits and
+// counts are cleared.  Returns the number of non-zero topics.
+template <class E>
+__device__ __forceinline__ uint32_t cta_compact(int bw, const Hist<true>& hist, uint32_t* bits, uint32_t* wsum,
+                                                const E& emit) {
+    const int R = (bw + blockDim.x - 1) / blockDim.x;
+    const int w0 = min(bw, (int)threadIdx.x * R), w1 = min(bw, w0 + R);
+    uint32_t c = 0;
+    for (int wi = w0; wi < w1; ++wi) c += (uint32_t)__popc(bits[wi]);
+    uint32_t total;
+    uint32_t p = cta_exclusive_scan(c, wsum, &total);
+    for (int wi = w0; wi < w1; ++wi) {
+        uint32_t m = bits[wi];
+        if (m) bits[wi] = 0u;
+        while (m) {
+            const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+            m &= m - 1u;
+            emit(k, hist.get(k), p++);
+            hist.clear(k);
+        }
+    }
+    return total;
+}
+
+// Word-topic rows above kLargeK topics: CTA per word tile (a dense word's chunk segment
+// of up to 16,384 tokens, or a sparse word over all chunks).  Shared memory: the
+// histogram, the bitmap, then a sparse word's chunk segments ([C] offsets, [C + 1] prefix
+// counts).  Topic totals are not accumulated here (k_topic_totals).
+__global__ void __launch_bounds__(kRebuildThreads, 8) k_wt_build_cta(WtArgs a) {
+    extern __shared__ uint32_t smu[];
+    __shared__ uint32_t wsum[kRebuildThreads / 32];
+    __shared__ int s_tile;
+    const int hw = Hist<true>::words(a.K), bw = wt_bit_words(a.K);
+    const Hist<true> hist{smu};
+    uint32_t* bits = smu + hw;
+    uint32_t* so = bits + bw;
+    uint32_t* pre = so + a.C;
+    const int lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < hw + bw; i += blockDim.x) smu[i] = 0u;
+    for (;;) {
+        __syncthreads();  // the previous tile is done with the shared state
+        if (threadIdx.x == 0) s_tile = (int)atomicAdd(a.tile_counter, 1u);
+        __syncthreads();
+        const int tile = s_tile;
+        if (tile >= a.ntiles) break;
+        const int4 t = a.tiles[tile];
+        const int w = t.x;
+        if (t.w & 1) {
+            const uint16_t* z = a.z + (uint32_t)t.y;
+            cta_hist((uint32_t)t.z, [&](uint32_t i) { return (uint32_t)__ldg(z + i); }, hist, bits, a.K, a.err);
+        } else {
+            // the word's segment in every chunk, and their prefix counts
+            if (threadIdx.x < 32) {
+                uint32_t carry = 0;
+                if (lane == 0) pre[0] = 0u;
+                for (int c0 = 0; c0 < a.C; c0 += 32) {
+                    const int c = c0 + lane;
+                    uint32_t cnt = 0;
+                    if (c < a.C) {
+                        const size_t idx = (size_t)c * a.V + w;
+                        so[c] = __ldg(a.seg_off + idx);
+                        cnt = __ldg(a.seg_cnt + idx);
+                    }
+                    uint32_t incl = cnt;
+#pragma unroll
+                    for (int off = 1; off < 32; off <<= 1) {
+                        const uint32_t v = __shfl_up_sync(FULL, incl, off);
+                        if (lane >= off) incl += v;
+                    }
+                    if (c < a.C) pre[c + 1] = carry + incl;
+                    carry += __shfl_sync(FULL, incl, 31);
+                }
+            }
+            __syncthreads();
+            const int C = a.C;
+            cta_hist(pre[C], [&](uint32_t i) {
+                // the chunk holding the word's i-th token: the last c with pre[c] <= i
+                int lo = 0, hi = C - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (pre[mid] <= i) lo = mid; else hi = mid - 1;
+                }
+                return (uint32_t)__ldg(a.z + so[lo] + (i - pre[lo]));
+            }, hist, bits, a.K, a.err);
+        }
+        __syncthreads();
+        if (t.w & 1) {
+            int* row = a.dwt + (size_t)w * a.K;
+            cta_compact(bw, hist, bits, wsum, [&](uint32_t k, uint32_t h, uint32_t) { atomicAdd(row + k, (int)h); });
+        } else {
+            const int s = w - a.Vd;
+            uint32_t* out = a.swt_ent + a.swt_off[s];
+            const uint32_t nnz = cta_compact(bw, hist, bits, wsum,
+                                             [&](uint32_t k, uint32_t h, uint32_t p) { out[p] = (k << 16) | h; });
+            if (threadIdx.x == 0) a.swt_nnz[s] = nnz;
+        }
+    }
+}
+
+// Topic totals n_k of the word tiles a.tiles (all words, or a word range): warp per tile,
+// counts privatised per CTA in shared memory (K words) and flushed once; without SHARED
+// (K words beyond the shared memory) the warps add to n_k directly.
+template <bool SHARED>
+__global__ void __launch_bounds__(256) k_topic_totals(WtArgs a) {
+    extern __shared__ uint32_t smu[];
+    const int lane = threadIdx.x & 31;
+    if (SHARED) {
+        for (int i = threadIdx.x; i < a.K; i += blockDim.x) smu[i] = 0u;
+        __syncthreads();
+    }
+    auto add = [&](const uint16_t* z, uint32_t n) {
+        for (uint32_t base = 0; base < n; base += 128) {
+            uint32_t k[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t i = base + 32u * s + lane;
+                k[s] = i < n ? (uint32_t)__ldg(z + i) : 0xffffffffu;
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if (base + 32u * s >= n) break;
+                // a topic >= K is reported by the rebuild; it is not counted here
+                const bool valid = k[s] < (uint32_t)a.K;
+                const uint32_t kk = valid ? k[s] : 0xfffffffeu;
+                const unsigned m = __match_any_sync(FULL, kk);
+                if (valid && lane == __ffs(m) - 1) {
+                    if (SHARED) atomicAdd(smu + kk, (uint32_t)__popc(m));
+                    else atomicAdd(a.n_k + kk, __popc(m));
+                }
+            }
+        }
+    };
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= a.ntiles) break;
+        const int4 t = a.tiles[tile];
+        if (t.w & 1) {
+            add(a.z + (uint32_t)t.y, (uint32_t)t.z);
+        } else {
+            for (int c0 = 0; c0 < a.C; c0 += 32) {
+                const int c = c0 + lane;
+                uint32_t so = 0, sc = 0;
+                if (c < a.C) {
+                    const size_t idx = (size_t)c * a.V + t.x;
+                    so = __ldg(a.seg_off + idx);
+                    sc = __ldg(a.seg_cnt + idx);
+                }
+                const int nc = min(32, a.C - c0);
+                for (int j = 0; j < nc; ++j) {
+                    const uint32_t o = __shfl_sync(FULL, so, j), n = __shfl_sync(FULL, sc, j);
+                    if (n) add(a.z + o, n);
+                }
+            }
+        }
+    }
+    if (SHARED) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
+            const uint32_t v = smu[k];
+            if (v) atomicAdd(a.n_k + k, (int)v);
+        }
+    }
+}
+
+// Doc rows: CTA per doc (the doc's tokens spread over the CTA's threads), the histogram
+// and bitmap shared.  Rows are ascending k; SKEW: keys are word-column slot indices (the
+// trainer's rows up to kLargeK topics), else topics.
+template <bool SKEW>
+__global__ void __launch_bounds__(kRebuildThreads, 8) k_dt_build_cta(DtArgs a) {
+    extern __shared__ uint32_t smu[];
+    __shared__ uint32_t wsum[kRebuildThreads / 32];
+    const int hw = Hist<true>::words(a.K), bw = dt_bit_words(a.K);
+    const Hist<true> hist{smu};
+    uint32_t* bits = smu + hw;
+    for (int i = threadIdx.x; i < hw + bw; i += blockDim.x) smu[i] = 0u;
+    for (uint32_t d = a.d_begin + blockIdx.x; d < a.d_end; d += gridDim.x) {
+        __syncthreads();  // the previous doc is done with the shared state
+        const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
+        const uint32_t* dpos = a.dtok_pos + (b - a.tok_base);
+        const uint32_t* dword = a.dtok_word + (b - a.tok_base);
+        const uint16_t* z = a.z;
+        cta_hist(n, [&](uint32_t i) { return (uint32_t)__ldg(z + __ldg(dpos + i)); }, hist, bits, a.K, a.err);
+        __syncthreads();
+        for (uint32_t base = 0; base < n; base += 4u * kRebuildThreads) {
+            uint32_t pos[4], t2[4];
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                const uint32_t i = base + (uint32_t)(s * kRebuildThreads) + threadIdx.x;
+                pos[s] = i < n ? __ldg(dpos + i) : 0xffffffffu;
+                t2[s] = i < n ? __ldg(dword + i) : 0u;
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s) t2[s] = pos[s] != 0xffffffffu ? __ldg(a.st_top2 + t2[s]) : 0u;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if (pos[s] == 0xffffffffu) continue;
+                const uint32_t k1 = t2[s] & 0xffffu, k2 = t2[s] >> 16;
+                const uint32_t c1 = k1 < (uint32_t)a.K ? hist.get(k1) : 0u, c2 = k2 < (uint32_t)a.K ? hist.get(k2) : 0u;
+                a.meta[pos[s] - a.tok_base] = (c2 << 16) | c1;
+            }
+        }
+        __syncthreads();
+        uint32_t* out = a.dt_ent + (__ldg(a.dt_off + d) - a.dt_base);
+        const uint32_t nnz =
+            cta_compact(bw, hist, bits, wsum, [&](uint32_t k, uint32_t h, uint32_t p) {
+                out[p] = ((SKEW ? (uint32_t)col_skew((int)k) : k) << 16) | h;
+            });
+        if (threadIdx.x == 0) a.dt_nnz[d] = nnz;
+    }
+}
+
 // Word statistics: warp per word.
 __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
     extern __shared__ float smf[];

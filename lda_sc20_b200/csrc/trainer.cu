@@ -83,7 +83,7 @@ struct lda_trainer {
     uint32_t *seg_off = nullptr, *seg_cnt = nullptr;
     int4 *s_tiles = nullptr, *w_tiles = nullptr;
     double *tile_ll = nullptr, *ll_dev = nullptr;
-    unsigned* tile_ctr = nullptr;         // [1 + 2C]: word-topic tiles, then per chunk sampler tiles (two kinds)
+    unsigned* tile_ctr = nullptr;         // [2 + 2C]: word-topic tiles, per chunk sampler tiles (two kinds), topic totals
     unsigned long long* ctr = nullptr;    // [kCounters]
     int* err = nullptr;
     double* ll_host = nullptr;            // pinned
@@ -91,6 +91,8 @@ struct lda_trainer {
     int64_t dt_cap = 0, swt_cap = 0;
     size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0, smem_dense = 0, smem_sparse = 0;
     size_t smem_stats_sparse = 0;
+    int grid_wt_cta = 0, grid_dt_cta = 0, grid_totals = 0;  // K > kLargeK: the CTA-per-unit rebuilds
+    size_t smem_wt_cta = 0, smem_dt_cta = 0, smem_totals = 0;
     int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_sample_ll = 0, grid_dense = 0, grid_sparse = 0;
     int grid_stats_sparse = 0;
 
@@ -525,7 +527,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.seg_off, (int64_t)T.C * V); ALLOC(T.seg_cnt, (int64_t)T.C * V);
     ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
-    ALLOC(T.tile_ctr, 1 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
+    ALLOC(T.tile_ctr, 2 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
     if (T.large) { ALLOC(T.recip, T.K); ALLOC(T.smooth, T.K); }
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
@@ -575,6 +577,26 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     if ((rc = occupancy_grid(wt_fn, 32 * T.warps_wt, T.smem_wt, T.num_sms, &T.grid_wt))) return rc;
     if ((rc = occupancy_grid((const void*)dev::k_word_stats, threads, T.smem_stats, T.num_sms, &T.grid_stats))) return rc;
     if ((rc = occupancy_grid(dt_fn, 32 * T.warps_dt, T.smem_dt, T.num_sms, &T.grid_dt))) return rc;
+    if (T.large) {
+        // the CTA-per-unit rebuilds: one shared histogram and bitmap (plus a sparse word's
+        // chunk segments), and the topic totals' per-CTA counts when K words fit
+        const size_t hist_b = ((size_t)dev::Hist<true>::words(T.K) + bitw) * 4;
+        T.smem_wt_cta = hist_b + (2 * (size_t)T.C + 1) * 4;
+        T.smem_dt_cta = hist_b;
+        T.smem_totals = (size_t)T.K * 4 <= (size_t)max_smem ? (size_t)T.K * 4 : 0;
+        if (T.smem_wt_cta > (size_t)max_smem)
+            return fail(LDA_ERR_ARG, "K=%d with %d chunks does not fit in shared memory (word-topic rebuild)", T.K, T.C);
+        const void* tot_fn = T.smem_totals ? (const void*)dev::k_topic_totals<true> : (const void*)dev::k_topic_totals<false>;
+        CUDA_TRY(raise_smem_limit((const void*)dev::k_wt_build_cta, T.smem_wt_cta));
+        CUDA_TRY(raise_smem_limit((const void*)dev::k_dt_build_cta<false>, T.smem_dt_cta));
+        CUDA_TRY(raise_smem_limit(tot_fn, T.smem_totals));
+        if ((rc = occupancy_grid((const void*)dev::k_wt_build_cta, dev::kRebuildThreads, T.smem_wt_cta, T.num_sms,
+                                 &T.grid_wt_cta)) ||
+            (rc = occupancy_grid((const void*)dev::k_dt_build_cta<false>, dev::kRebuildThreads, T.smem_dt_cta, T.num_sms,
+                                 &T.grid_dt_cta)) ||
+            (rc = occupancy_grid(tot_fn, 256, T.smem_totals, T.num_sms, &T.grid_totals)))
+            return rc;
+    }
     if (!T.large) {
         for (bool ll : {false, true}) CUDA_TRY(raise_smem_limit(sample_kernel(ll, T.K), T.smem_sample));
         const int st = 32 * T.swarps;
@@ -737,9 +759,23 @@ extern "C" int lda_update_wt(lda_trainer* t) {
         CUDA_TRY(cudaMemsetAsync(t->dwt, 0, sizeof(int) * (size_t)t->Vd * t->K, t->stream));
     }
     CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
-    const int grid = std::max(1, std::min(t->grid_wt, (a.ntiles + t->warps_wt - 1) / t->warps_wt));
-    dev::k_wt_build<true><<<grid, 32 * t->warps_wt, t->smem_wt, t->stream>>>(a);
-    CUDA_TRY(cudaGetLastError());
+    if (t->large) {
+        // rows by CTA per tile, then the totals over the same tiles
+        const int grid = std::max(1, std::min(t->grid_wt_cta, a.ntiles));
+        dev::k_wt_build_cta<<<grid, dev::kRebuildThreads, t->smem_wt_cta, t->stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+        dev::WtArgs at = a;
+        at.tile_counter = t->tile_ctr + 1 + 2 * t->C;
+        CUDA_TRY(cudaMemsetAsync(at.tile_counter, 0, sizeof(unsigned), t->stream));
+        const int gt = std::max(1, std::min(t->grid_totals, (a.ntiles + 7) / 8));
+        if (t->smem_totals) dev::k_topic_totals<true><<<gt, 256, t->smem_totals, t->stream>>>(at);
+        else dev::k_topic_totals<false><<<gt, 256, 0, t->stream>>>(at);
+        CUDA_TRY(cudaGetLastError());
+    } else {
+        const int grid = std::max(1, std::min(t->grid_wt, (a.ntiles + t->warps_wt - 1) / t->warps_wt));
+        dev::k_wt_build<true><<<grid, 32 * t->warps_wt, t->smem_wt, t->stream>>>(a);
+        CUDA_TRY(cudaGetLastError());
+    }
     t->end_stage();
     return LDA_OK;
 }
@@ -837,13 +873,30 @@ static dev::DtArgs dt_args(const lda_trainer* t, int chunk, int slot) {
     return a;
 }
 
-static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
-    const dev::DtArgs a = dt_args(t, chunk, slot);
+// The doc-topic rebuild of docs [a.d_begin, a.d_end): warp per doc, or above kLargeK
+// topics CTA per doc.
+#ifndef LDA_DT_CTA
+#define LDA_DT_CTA 0
+#endif
+static int launch_dt(const lda_trainer* t, const dev::DtArgs& a, cudaStream_t q) {
     const int64_t nd = a.d_end - a.d_begin;
-    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps_dt - 1) / t->warps_dt));
-    dev::k_dt_build<true><<<grid, 32 * t->warps_dt, t->smem_dt, q>>>(a);
+    if (t->large) {
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt_cta, nd));
+        dev::k_dt_build_cta<false><<<grid, dev::kRebuildThreads, t->smem_dt_cta, q>>>(a);
+    } else if (LDA_DT_CTA) {
+        const size_t smem = ((size_t)dev::Hist<true>::words(t->K) + (t->K + 31) / 32) * 4;
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)t->num_sms * 8, nd));
+        dev::k_dt_build_cta<true><<<grid, dev::kRebuildThreads, smem, q>>>(a);
+    } else {
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps_dt - 1) / t->warps_dt));
+        dev::k_dt_build<true><<<grid, 32 * t->warps_dt, t->smem_dt, q>>>(a);
+    }
     CUDA_TRY(cudaGetLastError());
     return LDA_OK;
+}
+
+static int dt_launch(lda_trainer* t, int chunk, int slot, cudaStream_t q) {
+    return launch_dt(t, dt_args(t, chunk, slot), q);
 }
 
 static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, int ll_mode) {
@@ -904,6 +957,37 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
         CUDA_TRY(cudaGetLastError());
     }
     t->chunk_sampled_ll[chunk] = ll_mode != 0;
+    return LDA_OK;
+}
+
+// Resident chunks [c0, c1) in one doc-topic rebuild launch and one sampler launch (the
+// chunks' docs and tiles are contiguous; up to kLargeK topics, one launch samples them all).
+#ifndef LDA_CHUNKS_PER_LAUNCH
+#define LDA_CHUNKS_PER_LAUNCH 1
+#endif
+static int dt_launch_group(lda_trainer* t, int c0, int c1, cudaStream_t q) {
+    dev::DtArgs a = dt_args(t, c0, 0);
+    a.d_end = (uint32_t)t->chunk_doc[c1];
+    return launch_dt(t, a, q);
+}
+
+static int sample_launch_group(lda_trainer* t, int c0, int c1, int ll_mode, cudaStream_t q) {
+    int rc;
+    if (t->large || c1 - c0 == 1) {
+        for (int ch = c0; ch < c1; ++ch)
+            if ((rc = sample_launch(t, ch, 0, ll_mode, q))) return rc;
+        return LDA_OK;
+    }
+    dev::SampleArgs a = sample_args(t, c0, 0, ll_mode);
+    a.ntiles = t->s_tile_base[c1] - t->s_tile_base[c0];
+    CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(unsigned), q));
+    if (a.ntiles > 0) {
+        const int cap = a.ll_mode ? t->grid_sample_ll : t->grid_sample;
+        const int grid = std::max(1, std::min(cap, (a.ntiles + t->swarps - 1) / t->swarps));
+        launch_sample(a.ll_mode != 0, t->K, grid, 32 * t->swarps, t->smem_sample, q, a);
+        CUDA_TRY(cudaGetLastError());
+    }
+    for (int ch = c0; ch < c1; ++ch) t->chunk_sampled_ll[ch] = ll_mode != 0;
     return LDA_OK;
 }
 
@@ -1011,10 +1095,16 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
     }
     if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2)) {
         // one stream, so that the stage events time each stage alone
-        for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
-            if ((rc = lda_update_dt(t, ch))) return rc;
-            if ((rc = lda_sample_chunk(t, ch, ll_mode))) return rc;
-            if (zout && (rc = copy_back(t, ch, t->stream, zout))) return rc;
+        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += LDA_CHUNKS_PER_LAUNCH) {
+            const int c1 = std::min(t->chunk_last, c0 + LDA_CHUNKS_PER_LAUNCH);
+            t->begin_stage(2);
+            if ((rc = dt_launch_group(t, c0, c1, t->stream))) return rc;
+            t->end_stage();
+            t->begin_stage(3);
+            if ((rc = sample_launch_group(t, c0, c1, ll_mode, t->stream))) return rc;
+            t->end_stage();
+            for (int ch = c0; ch < c1; ++ch)
+                if (zout && (rc = copy_back(t, ch, t->stream, zout))) return rc;
         }
     } else if (!t->streaming) {
         // chunk i of the range on work stream i mod 2: the next chunk's doc-topic rebuild
@@ -1030,11 +1120,13 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
         }
         CUDA_TRY(cudaEventRecord(t->ev_fork, t->stream));
         for (int i = 0; i < 2; ++i) CUDA_TRY(cudaStreamWaitEvent(t->work[i], t->ev_fork, 0));
-        for (int ch = t->chunk_first; ch < t->chunk_last; ++ch) {
-            cudaStream_t q = t->work[(ch - t->chunk_first) & 1];
-            if ((rc = dt_launch(t, ch, 0, q))) return rc;
-            if ((rc = sample_launch(t, ch, 0, ll_mode, q))) return rc;
-            if (zout && (rc = copy_back(t, ch, q, zout))) return rc;
+        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += LDA_CHUNKS_PER_LAUNCH) {
+            const int c1 = std::min(t->chunk_last, c0 + LDA_CHUNKS_PER_LAUNCH);
+            cudaStream_t q = t->work[((c0 - t->chunk_first) / LDA_CHUNKS_PER_LAUNCH) & 1];
+            if ((rc = dt_launch_group(t, c0, c1, q))) return rc;
+            if ((rc = sample_launch_group(t, c0, c1, ll_mode, q))) return rc;
+            for (int ch = c0; ch < c1; ++ch)
+                if (zout && (rc = copy_back(t, ch, q, zout))) return rc;
         }
         for (int i = 0; i < 2; ++i) {
             CUDA_TRY(cudaEventRecord(t->ev_join[i], t->work[i]));

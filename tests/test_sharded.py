@@ -279,6 +279,11 @@ def test_word_and_doc_sharding_on_one_gpu_match_single_trainer(K, over):
         t.set_word_range(*w)
     ct = c.chunk_tok()
     for it in range(5):
+        # the single trainer's word side of this sweep's starting topics
+        full.update_wt()
+        full.max_topic()
+        full.sync()
+        want = (full.topic_totals(), full.dense_wt(), full.sparse_wt(), full.word_stats())
         full.iterate(1, ll=True)
         for t in shards:
             t.update_wt()
@@ -294,6 +299,14 @@ def test_word_and_doc_sharding_on_one_gpu_match_single_trainer(K, over):
         for r in range(2):
             exs[r].unpack(recv, skip=r)
         torch.cuda.synchronize()
+        # every shard now holds the whole word side
+        for t in shards:
+            assert np.array_equal(t.topic_totals(), want[0])
+            assert np.array_equal(t.dense_wt(), want[1])
+            for x, y in zip(t.sparse_wt(), want[2]):
+                assert np.array_equal(x, y)
+            for x, y in zip(t.word_stats(), want[3]):
+                assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
         lls = []
         for t in shards:
             t.sweep_chunks(ll=True)
@@ -309,12 +322,3 @@ def test_word_and_doc_sharding_on_one_gpu_match_single_trainer(K, over):
         n = sum(x[1] for x in lls)
         fs, fn = full.loglik()
         assert n == fn and abs(s - fs) <= 1e-9 * abs(fs), (it, s, fs)
-    # the gathered word side is the single trainer's
-    full.update_wt()
-    full.max_topic()
-    full.sync()
-    for t in shards:
-        assert np.array_equal(t.topic_totals(), full.topic_totals())
-        assert np.array_equal(t.dense_wt(), full.dense_wt())
-        for x, y in zip(t.word_stats(), full.word_stats()):
-            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
