@@ -106,38 +106,6 @@ struct Hist<true> {
     __device__ __forceinline__ void clear(uint32_t k) const { reinterpret_cast<uint16_t*>(h)[k] = 0; }
 };
 
-// Histogram of topics topic_of(i, valid), i in [0, n), into the warp's shared `hist`; a
-// topic whose count leaves zero also gets its bit in `bits` (ceil(K/32) words).  Every
-// lane calls topic_of (valid is false past n, where it returns 0xffffffff), so it may use
-// warp collectives.  Four 32-token steps of loads are in flight together.
-template <class H, class F>
-__device__ __forceinline__ void warp_hist(uint32_t n, const F& topic_of, const H& hist, uint32_t* bits, int K,
-                                          int lane, int* err) {
-    for (uint32_t base = 0; base < n; base += 128) {
-        uint32_t k[4];
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            const uint32_t i = base + 32u * s + lane;
-            k[s] = topic_of(i < n ? i : n - 1, i < n);
-        }
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-            if (base + 32u * s >= n) break;
-            bool valid = k[s] != 0xffffffffu;
-            uint32_t kk = k[s];
-            if (valid && kk >= (uint32_t)K) {
-                atomicOr(err, 1);
-                valid = false;
-                kk = 0xfffffffeu;
-            }
-            const unsigned m = __match_any_sync(FULL, kk);
-            if (valid && lane == __ffs(m) - 1) {
-                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
-            }
-        }
-    }
-}
-
 // Histogram of topics z[start, start + cnt) into the warp's shared `hist`; a topic whose
 // count leaves zero also gets its bit in `bits` (ceil(K/32) words).  Four 32-token steps
 // of topic loads are in flight together.

@@ -46,10 +46,6 @@ struct WtArgs {
 // shared array, or the model's global totals).
 __device__ __forceinline__ int wt_bit_words(int K) { return (K + 31) >> 5; }
 
-#ifndef LDA_WT_FLAT
-#define LDA_WT_FLAT 0
-#endif
-
 template <class H>
 __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, const H& hist, uint32_t* bits, unsigned* nk,
                                         int lane) {
@@ -57,40 +53,6 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, const H& 
     if (t.w & 1) {
         hist_segment(a.z, (uint32_t)t.y, (uint32_t)t.z, hist, bits, a.K, lane, a.err);
     } else {
-#if LDA_WT_FLAT
-        // a sparse word's segments in up to 32 chunks at a time, taken as one token range:
-        // lane c holds chunk c's offset and the inclusive prefix of the counts, and each
-        // lane finds its token's chunk by a 5-step search over the lanes' prefixes, so the
-        // topic loads of all segments are in flight together
-        for (int c0 = 0; c0 < a.C; c0 += 32) {
-            const int c = c0 + lane;
-            uint32_t so = 0, sc = 0;
-            if (c < a.C) {
-                const size_t idx = (size_t)c * a.V + w;
-                so = __ldg(a.seg_off + idx);
-                sc = __ldg(a.seg_cnt + idx);
-            }
-            uint32_t incl = sc;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, off);
-                if (lane >= off) incl += v;
-            }
-            const uint32_t base_l = so - (incl - sc);  // z index of the lane's segment minus its first rank
-            const uint32_t n = __shfl_sync(FULL, incl, 31);
-            warp_hist(n, [&](uint32_t i, bool valid) {
-                // the first lane whose inclusive prefix exceeds i
-                int j = 0;
-#pragma unroll
-                for (int step = 16; step > 0; step >>= 1) {
-                    const uint32_t v = __shfl_sync(FULL, incl, j + step - 1);
-                    if (v <= i) j += step;
-                }
-                const uint32_t b = __shfl_sync(FULL, base_l, j);
-                return valid ? (uint32_t)__ldg(a.z + b + i) : 0xffffffffu;
-            }, hist, bits, a.K, lane, a.err);
-        }
-#else
         // a sparse word's segments in every chunk: lane c loads chunk c's offset and count
         for (int c0 = 0; c0 < a.C; c0 += 32) {
             const int c = c0 + lane;
@@ -106,7 +68,6 @@ __device__ __forceinline__ void wt_tile(const WtArgs& a, const int4 t, const H& 
                 if (n) hist_segment(a.z, o, n, hist, bits, a.K, lane, a.err);
             }
         }
-#endif
     }
     __syncwarp();
     const int words = wt_bit_words(a.K);

@@ -483,7 +483,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
-                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(1 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? nb(T.K, 4) : 0) +
+                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(2 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? nb(T.K, 4) : 0) +
                                  nb(1, 4);
         T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
     }
@@ -588,11 +588,11 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return fail(LDA_ERR_ARG, "K=%d with %d chunks does not fit in shared memory (word-topic rebuild)", T.K, T.C);
         const void* tot_fn = T.smem_totals ? (const void*)dev::k_topic_totals<true> : (const void*)dev::k_topic_totals<false>;
         CUDA_TRY(raise_smem_limit((const void*)dev::k_wt_build_cta, T.smem_wt_cta));
-        CUDA_TRY(raise_smem_limit((const void*)dev::k_dt_build_cta<false>, T.smem_dt_cta));
+        CUDA_TRY(raise_smem_limit((const void*)dev::k_dt_build_cta, T.smem_dt_cta));
         CUDA_TRY(raise_smem_limit(tot_fn, T.smem_totals));
         if ((rc = occupancy_grid((const void*)dev::k_wt_build_cta, dev::kRebuildThreads, T.smem_wt_cta, T.num_sms,
                                  &T.grid_wt_cta)) ||
-            (rc = occupancy_grid((const void*)dev::k_dt_build_cta<false>, dev::kRebuildThreads, T.smem_dt_cta, T.num_sms,
+            (rc = occupancy_grid((const void*)dev::k_dt_build_cta, dev::kRebuildThreads, T.smem_dt_cta, T.num_sms,
                                  &T.grid_dt_cta)) ||
             (rc = occupancy_grid(tot_fn, 256, T.smem_totals, T.num_sms, &T.grid_totals)))
             return rc;
@@ -875,18 +875,11 @@ static dev::DtArgs dt_args(const lda_trainer* t, int chunk, int slot) {
 
 // The doc-topic rebuild of docs [a.d_begin, a.d_end): warp per doc, or above kLargeK
 // topics CTA per doc.
-#ifndef LDA_DT_CTA
-#define LDA_DT_CTA 0
-#endif
 static int launch_dt(const lda_trainer* t, const dev::DtArgs& a, cudaStream_t q) {
     const int64_t nd = a.d_end - a.d_begin;
     if (t->large) {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt_cta, nd));
-        dev::k_dt_build_cta<false><<<grid, dev::kRebuildThreads, t->smem_dt_cta, q>>>(a);
-    } else if (LDA_DT_CTA) {
-        const size_t smem = ((size_t)dev::Hist<true>::words(t->K) + (t->K + 31) / 32) * 4;
-        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)t->num_sms * 8, nd));
-        dev::k_dt_build_cta<true><<<grid, dev::kRebuildThreads, smem, q>>>(a);
+        dev::k_dt_build_cta<<<grid, dev::kRebuildThreads, t->smem_dt_cta, q>>>(a);
     } else {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps_dt - 1) / t->warps_dt));
         dev::k_dt_build<true><<<grid, 32 * t->warps_dt, t->smem_dt, q>>>(a);
@@ -962,9 +955,6 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
 
 // Resident chunks [c0, c1) in one doc-topic rebuild launch and one sampler launch (the
 // chunks' docs and tiles are contiguous; up to kLargeK topics, one launch samples them all).
-#ifndef LDA_CHUNKS_PER_LAUNCH
-#define LDA_CHUNKS_PER_LAUNCH 1
-#endif
 static int dt_launch_group(lda_trainer* t, int c0, int c1, cudaStream_t q) {
     dev::DtArgs a = dt_args(t, c0, 0);
     a.d_end = (uint32_t)t->chunk_doc[c1];
@@ -1093,10 +1083,18 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
         if ((rc = lda_update_wt(t))) return rc;
         if ((rc = lda_max_topic(t))) return rc;
     }
+    // Resident sweeps without host copies take the chunk range in two groups up to kLargeK
+    // topics: a group's chunks share one rebuild launch and one sampler launch, so the
+    // sampler drains its tail twice per sweep instead of once per chunk (the K=1024 corpus,
+    // 8 chunks: 13.51 -> 13.38 ms per sweep; one group of all 8 took 13.78 ms, its
+    // rebuild's topics and rows no longer fitting in L2).  Above kLargeK a chunk's rows
+    // alone nearly fill L2, and with host copies each chunk's copy waits for its sampling
+    // only, so those keep one chunk per launch.
+    const int cpl = (zout || t->large) ? 1 : std::max(1, (t->chunk_last - t->chunk_first + 1) / 2);
     if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2)) {
         // one stream, so that the stage events time each stage alone
-        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += LDA_CHUNKS_PER_LAUNCH) {
-            const int c1 = std::min(t->chunk_last, c0 + LDA_CHUNKS_PER_LAUNCH);
+        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += cpl) {
+            const int c1 = std::min(t->chunk_last, c0 + cpl);
             t->begin_stage(2);
             if ((rc = dt_launch_group(t, c0, c1, t->stream))) return rc;
             t->end_stage();
@@ -1120,9 +1118,9 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
         }
         CUDA_TRY(cudaEventRecord(t->ev_fork, t->stream));
         for (int i = 0; i < 2; ++i) CUDA_TRY(cudaStreamWaitEvent(t->work[i], t->ev_fork, 0));
-        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += LDA_CHUNKS_PER_LAUNCH) {
-            const int c1 = std::min(t->chunk_last, c0 + LDA_CHUNKS_PER_LAUNCH);
-            cudaStream_t q = t->work[((c0 - t->chunk_first) / LDA_CHUNKS_PER_LAUNCH) & 1];
+        for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += cpl) {
+            const int c1 = std::min(t->chunk_last, c0 + cpl);
+            cudaStream_t q = t->work[((c0 - t->chunk_first) / cpl) & 1];
             if ((rc = dt_launch_group(t, c0, c1, q))) return rc;
             if ((rc = sample_launch_group(t, c0, c1, ll_mode, q))) return rc;
             for (int ch = c0; ch < c1; ++ch)
