@@ -106,6 +106,14 @@ struct Hist<true> {
     __device__ __forceinline__ void clear(uint32_t k) const { reinterpret_cast<uint16_t*>(h)[k] = 0; }
 };
 
+// One token of topic k into a histogram, and the topic's bit into the bitmap of non-zero
+// topics when its count leaves zero.  (Setting the bit for every token instead, so that
+// neither atomic's result is waited on, was no faster.)
+template <class H>
+__device__ __forceinline__ void hist_token(const H& hist, uint32_t* bits, uint32_t k) {
+    if (hist.add(k, 1u) == 0u) atomicOr(&bits[k >> 5], 1u << (k & 31u));
+}
+
 // Histogram of topics z[start, start + cnt) into the warp's shared `hist`; a topic whose
 // count leaves zero also gets its bit in `bits` (ceil(K/32) words).  Four 32-token steps
 // of topic loads are in flight together.
@@ -129,10 +137,7 @@ __device__ __forceinline__ void hist_segment(const uint16_t* __restrict__ z, uin
                 valid = false;
                 kk = 0xfffffffeu;
             }
-            const unsigned m = __match_any_sync(FULL, kk);
-            if (valid && lane == __ffs(m) - 1) {
-                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
-            }
+            if (valid) hist_token(hist, bits, kk);
         }
     }
 }

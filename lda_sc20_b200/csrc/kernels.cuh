@@ -82,7 +82,6 @@ __device__ __forceinline__ uint32_t cta_exclusive_scan(uint32_t v, uint32_t* wsu
 template <class F>
 __device__ __forceinline__ void cta_hist(uint32_t n, const F& topic_of, const Hist<true>& hist, uint32_t* bits, int K,
                                          int* err) {
-    const int lane = threadIdx.x & 31;
     for (uint32_t base = 0; base < n; base += 4u * kRebuildThreads) {
         uint32_t k[4];
 #pragma unroll
@@ -100,10 +99,7 @@ __device__ __forceinline__ void cta_hist(uint32_t n, const F& topic_of, const Hi
                 valid = false;
                 kk = 0xfffffffeu;
             }
-            const unsigned m = __match_any_sync(FULL, kk);
-            if (valid && lane == __ffs(m) - 1) {
-                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
-            }
+            if (valid) hist_token(hist, bits, kk);
         }
     }
 }
@@ -234,11 +230,8 @@ __global__ void __launch_bounds__(256) k_topic_totals(WtArgs a) {
                 // a topic >= K is reported by the rebuild; it is not counted here
                 const bool valid = k[s] < (uint32_t)a.K;
                 const uint32_t kk = valid ? k[s] : 0xfffffffeu;
-                const unsigned m = __match_any_sync(FULL, kk);
-                if (valid && lane == __ffs(m) - 1) {
-                    if (SHARED) atomicAdd(smu + kk, (uint32_t)__popc(m));
-                    else atomicAdd(a.n_k + kk, __popc(m));
-                }
+                if (valid && SHARED) atomicAdd(smu + kk, 1u);
+                if (valid && !SHARED) atomicAdd(a.n_k + kk, 1);
             }
         }
     };

@@ -205,8 +205,7 @@ __device__ __forceinline__ void fold_hist(uint32_t* hist, const FoldArgs& a, con
             k = init ? foldin_init(a.seed_lo, a.seed_hi, q.rid, pos, a.K) : (uint32_t)__ldcg(zsrc + q.tok_off + pos);
             if (k >= (uint32_t)a.K) k = 0;  // topics are written < K; keep the index in bounds
         }
-        const unsigned m = __match_any_sync(FULL, k);
-        if (valid && lane == __ffs(m) - 1) atomicAdd(&hist[k >> 1], (uint32_t)__popc(m) << ((k & 1u) << 4));
+        if (valid) atomicAdd(&hist[k >> 1], 1u << ((k & 1u) << 4));
     }
     __syncwarp();
 }

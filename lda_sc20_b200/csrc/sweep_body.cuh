@@ -17,8 +17,8 @@ namespace dev {
 
 // ---------------------------------------------------------------- WT rebuild
 // Warp per word tile: the tile's topics are histogrammed in a warp-private shared row
-// (match_any-aggregated shared atomics, so a word whose tokens share a topic costs one
-// atomic per distinct topic per 32 tokens).  Dense tiles add their row into the dense
+// with one shared atomic per token (aggregating a warp's equal topics with
+// __match_any_sync first made the rebuild 2.6x slower).  Dense tiles add their row into the dense
 // word-topic matrix; a sparse word (one tile over all chunks) is compacted to
 // (k<<16 | count) ascending k.  Topic totals n_k are privatised per CTA and flushed once.
 // Replaces WTDen_Update_Kernel, WT_Update_Kernel, sparseMatrixAdd and
@@ -242,10 +242,7 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& his
                 valid = false;
                 kk = 0xfffffffeu;
             }
-            const unsigned m = __match_any_sync(FULL, kk);
-            if (valid && lane == __ffs(m) - 1) {
-                if (hist.add(kk, (uint32_t)__popc(m)) == 0u) atomicOr(&bits[kk >> 5], 1u << (kk & 31u));
-            }
+            if (valid) hist_token(hist, bits, kk);
         }
     }
     __syncwarp();
