@@ -385,18 +385,22 @@ def run_ours(args, world, rank, local):
     # log-likelihood of the state after the K timed sweeps (one extra evaluation sweep)
     z_after = tr.topics()
     ll_mean = tr.iterate(1, ll=True)
-    # sweep time with the FP64 LL evaluated every sweep (LL mode evaluates S for all tokens)
-    tr.set_topics(z0)
-    tr.iteration = 0
-    torch.cuda.synchronize()
-    e2 = torch.cuda.Event(enable_timing=True)
-    e3 = torch.cuda.Event(enable_timing=True)
+    # sweep time with the FP64 LL evaluated every sweep (LL mode evaluates S for all tokens),
+    # beside plain sweeps over the same first sweeps (early sweeps cost more than the average)
     n_ll = max(1, min(args.steps, 10))
-    e2.record(stream)
-    tr.iterate(n_ll, ll=True)
-    e3.record(stream)
-    torch.cuda.synchronize()
-    ms_ll_sweep = e2.elapsed_time(e3) / n_ll
+    ll_ms = {}
+    for mode in (False, True):
+        tr.set_topics(z0)
+        tr.iteration = 0
+        torch.cuda.synchronize()
+        e2 = torch.cuda.Event(enable_timing=True)
+        e3 = torch.cuda.Event(enable_timing=True)
+        e2.record(stream)
+        tr.iterate(n_ll, ll=mode)
+        e3.record(stream)
+        torch.cuda.synchronize()
+        ll_ms[mode] = e2.elapsed_time(e3) / n_ll
+    ms_ll_sweep = ll_ms[True]
 
     # per-sweep device time over a fresh run of the same sweeps (diagnostic, not the metric)
     tr.set_topics(z0)
@@ -487,6 +491,8 @@ def run_ours(args, world, rank, local):
                     if streaming else "no (resident)"},
             "loglik_per_token": ll_mean,
             "ms_per_step_with_ll": ms_ll_sweep,
+            "ll_sweeps": {"sweeps": f"0-{n_ll - 1}", "plain_ms": ll_ms[False], "with_ll_ms": ll_ms[True],
+                          "ll_cost": ll_ms[True] / ll_ms[False] - 1.0},
             "e2e": e2e,
             "gpu_launches": tm_launches,
             "roofline": {"bound": "hbm", "kernel": "k_sample", "achieved": achieved, "peak": peak,

@@ -205,6 +205,121 @@ __global__ void __launch_bounds__(kRebuildThreads, 8) k_wt_build_cta(WtArgs a) {
     }
 }
 
+// Rows of small sparse words above kLargeK topics (at most kSmallSparse tokens, over at
+// most 32 chunks): warp per word, without a histogram.  The warp holds the word's topics
+// in registers (up to 8 per lane), marks them in a bitmap, gives each topic its rank among
+// the word's distinct topics (the popcount prefix of the bitmap), counts per rank, and
+// writes the row ascending k.  Per warp: bitmap (bw words), prefix (bw uint16) and counts
+// (kSmallSparse words).  Rows equal k_wt_build_cta's.
+constexpr int kSmallSparse = 256;
+__host__ __device__ __forceinline__ size_t wt_small_warp_words(int K) {
+    const size_t bw = (size_t)(K + 31) >> 5;
+    return bw + ((bw + 1) >> 1) + kSmallSparse;
+}
+__global__ void __launch_bounds__(256) k_wt_sparse_small(WtArgs a) {
+    extern __shared__ uint32_t smu[];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bw = wt_bit_words(a.K);
+    uint32_t* bits = smu + wt_small_warp_words(a.K) * wid;
+    uint16_t* pre = reinterpret_cast<uint16_t*>(bits + bw);
+    uint32_t* cnt = bits + bw + ((bw + 1) >> 1);
+    for (int i = lane; i < bw; i += 32) bits[i] = 0u;
+    for (int i = lane; i < kSmallSparse; i += 32) cnt[i] = 0u;
+    __syncwarp();
+    for (;;) {
+        int tile = 0;
+        if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(FULL, tile, 0);
+        if (tile >= a.ntiles) break;
+        const int w = a.tiles[tile].x;
+        // lane c: chunk c's segment of the word, as z index minus the segment's first rank
+        uint32_t so = 0, sc = 0;
+        if (lane < a.C) {
+            const size_t idx = (size_t)lane * a.V + w;
+            so = __ldg(a.seg_off + idx);
+            sc = __ldg(a.seg_cnt + idx);
+        }
+        uint32_t incl = sc;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t v = __shfl_up_sync(FULL, incl, off);
+            if (lane >= off) incl += v;
+        }
+        const uint32_t base_l = so - (incl - sc);
+        const uint32_t n = min(__shfl_sync(FULL, incl, 31), (uint32_t)kSmallSparse);
+        uint32_t k[kSmallSparse / 32];
+#pragma unroll
+        for (int j = 0; j < kSmallSparse / 32; ++j) {
+            const uint32_t i = 32u * (uint32_t)j + (uint32_t)lane;
+            k[j] = 0xffffffffu;
+            if (32u * (uint32_t)j >= n) continue;  // uniform
+            // the first lane whose inclusive prefix exceeds i
+            const uint32_t ii = i < n ? i : n - 1;
+            int c = 0;
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1) {
+                const uint32_t v = __shfl_sync(FULL, incl, c + step - 1);
+                if (v <= ii) c += step;
+            }
+            const uint32_t b = __shfl_sync(FULL, base_l, c);
+            if (i < n) {
+                uint32_t kk = (uint32_t)__ldg(a.z + b + i);
+                if (kk >= (uint32_t)a.K) {
+                    atomicOr(a.err, 1);
+                    kk = 0xffffffffu;
+                }
+                k[j] = kk;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kSmallSparse / 32; ++j)
+            if (k[j] != 0xffffffffu) atomicOr(&bits[k[j] >> 5], 1u << (k[j] & 31u));
+        __syncwarp();
+        uint32_t carry = 0;
+        for (int wb = 0; wb < bw; wb += 32) {
+            const int wi = wb + lane;
+            const uint32_t c = wi < bw ? (uint32_t)__popc(bits[wi]) : 0u;
+            uint32_t inc = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, inc, off);
+                if (lane >= off) inc += v;
+            }
+            if (wi < bw) pre[wi] = (uint16_t)(carry + inc - c);
+            carry += __shfl_sync(FULL, inc, 31);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < kSmallSparse / 32; ++j) {
+            const uint32_t kk = k[j];
+            if (kk != 0xffffffffu) {
+                const uint32_t m = bits[kk >> 5];
+                atomicAdd(&cnt[pre[kk >> 5] + __popc(m & ((1u << (kk & 31u)) - 1u))], 1u);
+            }
+        }
+        __syncwarp();
+        const int s = w - a.Vd;
+        uint32_t* out = a.swt_ent + a.swt_off[s];
+        for (int wb = 0; wb < bw; wb += 32) {
+            const int wi = wb + lane;
+            uint32_t m = wi < bw ? bits[wi] : 0u;
+            if (m) {
+                bits[wi] = 0u;
+                uint32_t p = pre[wi];
+                while (m) {
+                    const uint32_t kk = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+                    m &= m - 1u;
+                    out[p] = (kk << 16) | cnt[p];
+                    cnt[p] = 0u;
+                    ++p;
+                }
+            }
+        }
+        if (lane == 0) a.swt_nnz[s] = carry;
+        __syncwarp();
+    }
+}
+
 // Topic totals n_k of the word tiles a.tiles (all words, or a word range): warp per tile,
 // counts privatised per CTA in shared memory (K words) and flushed once; without SHARED
 // (K words beyond the shared memory) the warps add to n_k directly.

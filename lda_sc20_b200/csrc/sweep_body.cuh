@@ -406,7 +406,7 @@ constexpr int kSampleWarps = LDA_SAMPLE_WARPS;
 #define LDA_SAMPLE_QB_MIN_BLOCKS 4
 #endif
 #ifndef LDA_SAMPLE_LL_MIN_BLOCKS
-#define LDA_SAMPLE_LL_MIN_BLOCKS 4
+#define LDA_SAMPLE_LL_MIN_BLOCKS 5
 #endif
 #ifndef LDA_SPARSE_LARGE_MIN_BLOCKS
 #define LDA_SPARSE_LARGE_MIN_BLOCKS 4

@@ -83,7 +83,7 @@ struct lda_trainer {
     uint32_t *seg_off = nullptr, *seg_cnt = nullptr;
     int4 *s_tiles = nullptr, *w_tiles = nullptr;
     double *tile_ll = nullptr, *ll_dev = nullptr;
-    unsigned* tile_ctr = nullptr;         // [2 + 2C]: word-topic tiles, per chunk sampler tiles (two kinds), topic totals
+    unsigned* tile_ctr = nullptr;         // [3 + 2C]: word-topic tiles, per chunk sampler tiles (two kinds), topic totals, small sparse words
     unsigned long long* ctr = nullptr;    // [kCounters]
     int* err = nullptr;
     double* ll_host = nullptr;            // pinned
@@ -113,6 +113,11 @@ struct lda_trainer {
     int32_t wt_lo = 0, wt_hi = 0;
     int4* w_tiles_rng = nullptr;
     int n_wtiles_rng = 0;
+    // K > kLargeK: the last n_wsmall word tiles (n_wsmall_rng of a range's) are sparse words of at
+    // most dev::kSmallSparse tokens, built warp per word by k_wt_sparse_small
+    int n_wsmall = 0, n_wsmall_rng = 0;
+    int grid_wsmall = 0;
+    size_t smem_wsmall = 0;
 
     // streaming: the per-token arrays of the doc-topic rebuild and the sampler (doc of each
     // token, doc-order -> word-sorted map and word, per-token metadata) and the doc rows
@@ -462,6 +467,12 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         }
     }
     std::stable_sort(wt.begin(), wt.end(), [](const int4& a, const int4& b) { return a.z > b.z; });
+    if (T.large && T.C <= 32) {
+        // small sparse words last (stable: each part keeps largest first)
+        auto big = [&](const int4& x) { return (x.w & 1) || x.z > dev::kSmallSparse; };
+        const auto mid = std::stable_partition(wt.begin(), wt.end(), big);
+        T.n_wsmall = (int)(wt.end() - mid);
+    }
     T.n_wtiles = (int)wt.size();
 
     // ---- resident or streamed chunks (EZLDA streams every chunk through fixed buffers,
@@ -483,7 +494,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
-                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(2 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? nb(T.K, 4) : 0) +
+                                 nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(3 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? nb(T.K, 4) : 0) +
                                  nb(1, 4);
         T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
     }
@@ -527,7 +538,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.seg_off, (int64_t)T.C * V); ALLOC(T.seg_cnt, (int64_t)T.C * V);
     ALLOC(T.s_tiles, (int64_t)st.size()); ALLOC(T.w_tiles, (int64_t)wt.size());
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
-    ALLOC(T.tile_ctr, 2 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
+    ALLOC(T.tile_ctr, 3 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
     if (T.large) { ALLOC(T.recip, T.K); ALLOC(T.smooth, T.K); }
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
@@ -588,6 +599,16 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return fail(LDA_ERR_ARG, "K=%d with %d chunks does not fit in shared memory (word-topic rebuild)", T.K, T.C);
         const void* tot_fn = T.smem_totals ? (const void*)dev::k_topic_totals<true> : (const void*)dev::k_topic_totals<false>;
         CUDA_TRY(raise_smem_limit((const void*)dev::k_wt_build_cta, T.smem_wt_cta));
+        T.smem_wsmall = dev::wt_small_warp_words(T.K) * 4 * 8;
+        if (T.n_wsmall > 0) {
+            if (T.smem_wsmall > (size_t)max_smem) {
+                T.n_wsmall = 0;  // the CTA kernel takes every tile
+            } else {
+                CUDA_TRY(raise_smem_limit((const void*)dev::k_wt_sparse_small, T.smem_wsmall));
+                if ((rc = occupancy_grid((const void*)dev::k_wt_sparse_small, 256, T.smem_wsmall, T.num_sms, &T.grid_wsmall)))
+                    return rc;
+            }
+        }
         CUDA_TRY(raise_smem_limit((const void*)dev::k_dt_build_cta, T.smem_dt_cta));
         CUDA_TRY(raise_smem_limit(tot_fn, T.smem_totals));
         if ((rc = occupancy_grid((const void*)dev::k_wt_build_cta, dev::kRebuildThreads, T.smem_wt_cta, T.num_sms,
@@ -678,6 +699,8 @@ extern "C" int lda_trainer_set_word_range(lda_trainer* t, int32_t w0, int32_t w1
     CUDA_TRY(cudaMalloc(&t->w_tiles_rng, sizeof(int4) * std::max<size_t>(r.size(), 1)));
     if (!r.empty()) CUDA_TRY(cudaMemcpy(t->w_tiles_rng, r.data(), sizeof(int4) * r.size(), cudaMemcpyHostToDevice));
     t->n_wtiles_rng = (int)r.size();
+    t->n_wsmall_rng = 0;
+    for (const int4& x : r) t->n_wsmall_rng += t->n_wsmall > 0 && !(x.w & 1) && x.z <= dev::kSmallSparse;
     return LDA_OK;
 }
 
@@ -760,10 +783,26 @@ extern "C" int lda_update_wt(lda_trainer* t) {
     }
     CUDA_TRY(cudaMemsetAsync(t->tile_ctr, 0, sizeof(unsigned), t->stream));
     if (t->large) {
-        // rows by CTA per tile, then the totals over the same tiles
-        const int grid = std::max(1, std::min(t->grid_wt_cta, a.ntiles));
-        dev::k_wt_build_cta<<<grid, dev::kRebuildThreads, t->smem_wt_cta, t->stream>>>(a);
-        CUDA_TRY(cudaGetLastError());
+        // rows by CTA per tile (small sparse words by warp per word), then the totals over
+        // the same tiles
+        const int nsmall = t->w_tiles_rng ? t->n_wsmall_rng : t->n_wsmall;
+        dev::WtArgs ab = a;
+        ab.ntiles = a.ntiles - nsmall;
+        if (ab.ntiles > 0) {
+            const int grid = std::max(1, std::min(t->grid_wt_cta, ab.ntiles));
+            dev::k_wt_build_cta<<<grid, dev::kRebuildThreads, t->smem_wt_cta, t->stream>>>(ab);
+            CUDA_TRY(cudaGetLastError());
+        }
+        if (nsmall > 0) {
+            dev::WtArgs as = a;
+            as.tiles = a.tiles + ab.ntiles;
+            as.ntiles = nsmall;
+            as.tile_counter = t->tile_ctr + 2 + 2 * t->C;
+            CUDA_TRY(cudaMemsetAsync(as.tile_counter, 0, sizeof(unsigned), t->stream));
+            const int grid = std::max(1, std::min(t->grid_wsmall, (nsmall + 7) / 8));
+            dev::k_wt_sparse_small<<<grid, 256, t->smem_wsmall, t->stream>>>(as);
+            CUDA_TRY(cudaGetLastError());
+        }
         dev::WtArgs at = a;
         at.tile_counter = t->tile_ctr + 1 + 2 * t->C;
         CUDA_TRY(cudaMemsetAsync(at.tile_counter, 0, sizeof(unsigned), t->stream));
