@@ -52,6 +52,7 @@ __global__ void __launch_bounds__(256) k_wt_build(WtArgs a) {
 // errors are those of k_wt_build / k_dt_build, bit for bit; the topic totals come from
 // k_topic_totals.
 constexpr int kRebuildThreads = 256;
+constexpr int kSmoothMaxRounds = 2048;  // rounds of 32 topics in the smoothing table (K <= 65,536)
 
 // Exclusive scan of one value per thread across the CTA; *total gets the sum.  wsum holds
 // a word per warp.  Every thread of the CTA calls it.
@@ -398,6 +399,7 @@ __global__ void __launch_bounds__(kRebuildThreads, 8) k_dt_build_cta(DtArgs a) {
     for (uint32_t d = a.d_begin + blockIdx.x; d < a.d_end; d += gridDim.x) {
         __syncthreads();  // the previous doc is done with the shared state
         const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
+        if (n <= a.small_max) continue;  // k_dt_build_small's doc
         const uint32_t* dpos = a.dtok_pos + (b - a.tok_base);
         const uint32_t* dword = a.dtok_word + (b - a.tok_base);
         const uint16_t* z = a.z;
@@ -429,6 +431,114 @@ __global__ void __launch_bounds__(kRebuildThreads, 8) k_dt_build_cta(DtArgs a) {
     }
 }
 
+// Doc rows above kLargeK topics for docs of at most a.small_max (<= kSmallDoc) tokens:
+// warp per doc, without a histogram (as k_wt_sparse_small builds small words' rows).  The
+// warp holds the doc's topics in registers, marks them in a bitmap, ranks each topic among
+// the doc's distinct topics by the bitmap's popcount prefix and counts per rank; a topic's
+// count is then one bitmap test and one lookup, for the tokens' metadata and the row.
+// Rows, metadata and errors equal k_dt_build_cta's.
+constexpr int kSmallDoc = 384;
+__host__ __device__ __forceinline__ size_t dt_small_warp_words(int K) {
+    const size_t bw = (size_t)(K + 31) >> 5;
+    return bw + ((bw + 1) >> 1) + kSmallDoc;
+}
+#ifndef LDA_DT_SMALL_MIN_BLOCKS
+#define LDA_DT_SMALL_MIN_BLOCKS 6
+#endif
+__global__ void __launch_bounds__(256, LDA_DT_SMALL_MIN_BLOCKS) k_dt_build_small(DtArgs a) {
+    extern __shared__ uint32_t smu[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bw = dt_bit_words(a.K);
+    uint32_t* bits = smu + dt_small_warp_words(a.K) * wid;
+    uint16_t* pre = reinterpret_cast<uint16_t*>(bits + bw);
+    uint32_t* cnt = bits + bw + ((bw + 1) >> 1);
+    for (int i = lane; i < bw; i += 32) bits[i] = 0u;
+    for (int i = lane; i < kSmallDoc; i += 32) cnt[i] = 0u;
+    __syncwarp();
+    // the doc's count of topic k (bits, pre and cnt complete)
+    auto count_of = [&](uint32_t k) -> uint32_t {
+        if (k >= (uint32_t)a.K) return 0u;
+        const uint32_t m = bits[k >> 5], sh = k & 31u;
+        return (m >> sh) & 1u ? cnt[pre[k >> 5] + __popc(m & ((1u << sh) - 1u))] : 0u;
+    };
+    for (uint32_t d = a.d_begin + blockIdx.x * warps + wid; d < a.d_end; d += gridDim.x * warps) {
+        const uint32_t b = __ldg(a.doc_off + d), n = __ldg(a.doc_off + d + 1) - b;
+        if (n > a.small_max) continue;  // k_dt_build_cta's doc
+        const uint32_t* dpos = a.dtok_pos + (b - a.tok_base);
+        const uint32_t* dword = a.dtok_word + (b - a.tok_base);
+        uint32_t k[kSmallDoc / 32];
+#pragma unroll
+        for (int j = 0; j < kSmallDoc / 32; ++j) {
+            const uint32_t i = 32u * (uint32_t)j + (uint32_t)lane;
+            k[j] = i < n ? __ldg(dpos + i) : 0xffffffffu;
+        }
+#pragma unroll
+        for (int j = 0; j < kSmallDoc / 32; ++j) {
+            if (k[j] == 0xffffffffu) continue;
+            uint32_t kk = (uint32_t)__ldg(a.z + k[j]);
+            if (kk >= (uint32_t)a.K) {
+                atomicOr(a.err, 1);
+                kk = 0xffffffffu;
+            }
+            k[j] = kk;
+        }
+#pragma unroll
+        for (int j = 0; j < kSmallDoc / 32; ++j)
+            if (k[j] != 0xffffffffu) atomicOr(&bits[k[j] >> 5], 1u << (k[j] & 31u));
+        __syncwarp();
+        uint32_t carry = 0;
+        for (int wb = 0; wb < bw; wb += 32) {
+            const int wi = wb + lane;
+            const uint32_t c = wi < bw ? (uint32_t)__popc(bits[wi]) : 0u;
+            uint32_t inc = c;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const uint32_t v = __shfl_up_sync(FULL, inc, off);
+                if (lane >= off) inc += v;
+            }
+            if (wi < bw) pre[wi] = (uint16_t)(carry + inc - c);
+            carry += __shfl_sync(FULL, inc, 31);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < kSmallDoc / 32; ++j) {
+            const uint32_t kk = k[j];
+            if (kk != 0xffffffffu) {
+                const uint32_t m = bits[kk >> 5];
+                atomicAdd(&cnt[pre[kk >> 5] + __popc(m & ((1u << (kk & 31u)) - 1u))], 1u);
+            }
+        }
+        __syncwarp();
+        // each token's counts of its word's max and 2nd topics
+        for (uint32_t base = 0; base < n; base += 32) {
+            const uint32_t i = base + (uint32_t)lane;
+            if (i < n) {
+                const uint32_t pos = __ldg(dpos + i), t2 = __ldg(a.st_top2 + __ldg(dword + i));
+                a.meta[pos - a.tok_base] = (count_of(t2 >> 16) << 16) | count_of(t2 & 0xffffu);
+            }
+        }
+        __syncwarp();
+        uint32_t* out = a.dt_ent + (__ldg(a.dt_off + d) - a.dt_base);
+        for (int wb = 0; wb < bw; wb += 32) {
+            const int wi = wb + lane;
+            uint32_t m = wi < bw ? bits[wi] : 0u;
+            if (m) {
+                bits[wi] = 0u;
+                uint32_t p = pre[wi];
+                while (m) {
+                    const uint32_t kk = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
+                    m &= m - 1u;
+                    out[p] = (kk << 16) | cnt[p];
+                    cnt[p] = 0u;
+                    ++p;
+                }
+            }
+        }
+        if (lane == 0) a.dt_nnz[d] = carry;
+        __syncwarp();
+    }
+}
+
 // Word statistics: warp per word.
 __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
     extern __shared__ float smf[];
@@ -440,6 +550,19 @@ __global__ void __launch_bounds__(256) k_word_stats(StatsArgs a) {
     for (int w = a.wlo + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
         word_stats_word(a, w, r, col, lane);
     }
+}
+
+// Word statistics of dense words above kLargeK topics: warp per word, phi formed on the fly
+// from the word's count row and the CTA's reciprocals (no K-wide column per warp, which
+// left 4 warps per SM at K=10,000).  Results equal k_word_stats'.
+__global__ void __launch_bounds__(256) k_word_stats_dense_rows(StatsArgs a) {
+    extern __shared__ float smf[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* r = smf;
+    fill_recip(r, a.n_k, a.K, a.Vbeta);
+    __syncthreads();
+    for (int w = a.wlo + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps)
+        word_stats_from(a, w, DenseRowPhi{a.dwt + (size_t)w * a.K, r, a.beta}, lane);
 }
 
 // Doc-topic rebuild: warp per doc of one chunk.  P16: 16-bit histogram counts (a doc has
@@ -864,19 +987,33 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
 
 // The smoothing table of the split Q bucket (K > kLargeK): T[k] = carry + Kogge-Stone scan
 // of sm_k = alpha * (beta * r_k) over rounds of 32 topics, the carry being the previous
-// round's last prefix, so T is non-decreasing and T[K-1] is the total.  One warp; r_k is
-// formed from n_k as fill_recip forms it.
-__global__ void __launch_bounds__(32) k_smooth_table(const int* __restrict__ n_k, int K, float Vbeta, float alpha,
-                                                     float beta, float* __restrict__ T) {
-    const int lane = threadIdx.x;
-    float carry = 0.0f;
-    for (int base = 0; base < K; base += 32) {
-        const int k = base + lane;
+// round's last prefix, so T is non-decreasing and T[K-1] is the total.  r_k is formed from
+// n_k as fill_recip forms it.  One CTA: its warps scan the rounds in parallel (the scan of
+// a round does not depend on the carry), one thread chains the carries, then every T[k] is
+// one addition.  T holds each round's scan until the carries are known.
+__global__ void __launch_bounds__(1024) k_smooth_table(const int* __restrict__ n_k, int K, float Vbeta, float alpha,
+                                                       float beta, float* __restrict__ T) {
+    __shared__ float carry_s[kSmoothMaxRounds];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rounds = (K + 31) >> 5;
+    for (int rd = wid; rd < rounds; rd += warps) {
+        const int k = 32 * rd + lane;
         const float sm = k < K ? fmul(alpha, fmul(beta, __fdiv_rn(1.0f, fadd(__int2float_rn(n_k[k]), Vbeta)))) : 0.0f;
-        const float P = fadd(carry, warp_ks_scan(sm, lane));
-        if (k < K) T[k] = P;
-        carry = __shfl_sync(FULL, P, 31);
+        const float sc = warp_ks_scan(sm, lane);
+        if (k < K) T[k] = sc;
+        if (lane == 31) carry_s[rd] = sc;  // the round's total for now
     }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        float carry = 0.0f;
+        for (int rd = 0; rd < rounds; ++rd) {
+            const float tot = carry_s[rd];
+            carry_s[rd] = carry;
+            carry = fadd(carry, tot);
+        }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < K; k += blockDim.x) T[k] = fadd(carry_s[k >> 5], T[k]);
 }
 
 // r_k = 1 / ((float)n_k + V*beta), the value fill_recip forms, into a global table.

@@ -137,14 +137,38 @@ struct StatsArgs {
 };
 
 // Statistics of word w from its column (built into the warp's shared `col`).
+// phi_k of dense word w formed on the fly from its count row, the value build_column stores
+struct DenseRowPhi {
+    const int* row;
+    const float* r;
+    float beta;
+    __device__ __forceinline__ float operator()(int k) const {
+        return fmul(fadd(__int2float_rn(__ldg(row + k)), beta), r[k]);
+    }
+};
+struct ColumnPhi {
+    const float* col;
+    __device__ __forceinline__ float operator()(int k) const { return col[k]; }
+};
+
+// The statistics of word w from phi(k), k < K: top three, the lane partials of Q (the
+// max topic excluded) and Q.
+template <class Phi>
+__device__ __forceinline__ void word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane);
+
 __device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const float* r, float* col, int lane) {
     build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, nullptr);
+    word_stats_from(a, w, ColumnPhi{col}, lane);
+}
+
+template <class Phi>
+__device__ __forceinline__ void word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane) {
     // the lane's top three by (phi desc, k asc) in one pass (k ascends, so a strictly larger
     // value is needed to displace), then three warp-wide pops of the lanes' heads
     float a1 = -1.0f, a2 = -1.0f, a3 = -1.0f;
     int i1 = 0x7fffffff, i2 = 0x7fffffff, i3 = 0x7fffffff;
     for (int k = lane; k < a.K; k += 32) {
-        const float x = col[k];
+        const float x = phi(k);
         if (x > a1) {
             a3 = a2; i3 = i2;
             a2 = a1; i2 = i1;
@@ -174,7 +198,7 @@ __device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const
     const float v1 = v[0], v2 = v[1], v3 = v[2];
     const int k1 = kk[0], k2 = kk[1], k3 = kk[2];
     float ql = 0.0f;
-    for (int k = lane; k < a.K; k += 32) if (k != k1) ql = ffma(a.alpha, col[k], ql);
+    for (int k = lane; k < a.K; k += 32) if (k != k1) ql = ffma(a.alpha, phi(k), ql);
     const float qp = warp_ks_scan(ql, lane);
     const float Q = __shfl_sync(FULL, qp, 31);
     a.st_ql[(size_t)w * 32 + lane] = ql;
@@ -209,6 +233,9 @@ struct DtArgs {
     // entries [dt_base, ...): 0 when the whole corpus is resident, the chunk's first token
     // and first doc-row entry when the chunk is streamed into a slot buffer
     uint32_t tok_base, dt_base;
+    // above kLargeK topics: docs of at most small_max tokens are k_dt_build_small's, the
+    // rest k_dt_build_cta's (0: all the CTA kernel's)
+    uint32_t small_max = 0;
 };
 
 // Doc d: its counts in the warp's shared `hist` (K words) and the bitmap of its non-zero

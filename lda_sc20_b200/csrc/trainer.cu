@@ -92,6 +92,9 @@ struct lda_trainer {
     size_t smem_wt = 0, smem_stats = 0, smem_dt = 0, smem_sample = 0, smem_dense = 0, smem_sparse = 0;
     size_t smem_stats_sparse = 0;
     int grid_wt_cta = 0, grid_dt_cta = 0, grid_totals = 0;  // K > kLargeK: the CTA-per-unit rebuilds
+    int grid_stats_dense = 0;                                // K > kLargeK: dense-word statistics
+    int grid_dt_small = 0;                                   // K > kLargeK: docs of few tokens, warp per doc
+    size_t smem_dt_small = 0;
     size_t smem_wt_cta = 0, smem_dt_cta = 0, smem_totals = 0;
     int grid_wt = 0, grid_stats = 0, grid_dt = 0, grid_sample = 0, grid_sample_ll = 0, grid_dense = 0, grid_sparse = 0;
     int grid_stats_sparse = 0;
@@ -599,6 +602,12 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return fail(LDA_ERR_ARG, "K=%d with %d chunks does not fit in shared memory (word-topic rebuild)", T.K, T.C);
         const void* tot_fn = T.smem_totals ? (const void*)dev::k_topic_totals<true> : (const void*)dev::k_topic_totals<false>;
         CUDA_TRY(raise_smem_limit((const void*)dev::k_wt_build_cta, T.smem_wt_cta));
+        T.smem_dt_small = dev::dt_small_warp_words(T.K) * 4 * 8;
+        if (T.smem_dt_small <= (size_t)max_smem) {
+            CUDA_TRY(raise_smem_limit((const void*)dev::k_dt_build_small, T.smem_dt_small));
+            if ((rc = occupancy_grid((const void*)dev::k_dt_build_small, 256, T.smem_dt_small, T.num_sms, &T.grid_dt_small)))
+                return rc;
+        }
         T.smem_wsmall = dev::wt_small_warp_words(T.K) * 4 * 8;
         if (T.n_wsmall > 0) {
             if (T.smem_wsmall > (size_t)max_smem) {
@@ -637,6 +646,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
             return rc;
         T.grid_dense = std::min(g0, g1);
         T.grid_sparse = std::min(g2, g3);
+        CUDA_TRY(raise_smem_limit((const void*)dev::k_word_stats_dense_rows, (size_t)T.K * 4));
+        if ((rc = occupancy_grid((const void*)dev::k_word_stats_dense_rows, 256, (size_t)T.K * 4, T.num_sms,
+                                 &T.grid_stats_dense)))
+            return rc;
         T.smem_stats_sparse = dev::stats_sparse_smem(T.K, kLargeWarps);
         CUDA_TRY(raise_smem_limit((const void*)dev::k_word_stats_sparse_large, T.smem_stats_sparse));
         if ((rc = occupancy_grid((const void*)dev::k_word_stats_sparse_large, lt, T.smem_stats_sparse, T.num_sms,
@@ -837,14 +850,14 @@ extern "C" int lda_max_topic(lda_trainer* t) {
         }
     } else {
         // the smoothing table of the sparse words' split Q bucket, then dense words from
-        // their columns, sparse words without one
-        dev::k_smooth_table<<<1, 32, 0, t->stream>>>(t->n_k, t->K, t->Vbeta, t->alpha, t->beta, t->smooth);
+        // their count rows, sparse words from their entries
+        dev::k_smooth_table<<<1, 1024, 0, t->stream>>>(t->n_k, t->K, t->Vbeta, t->alpha, t->beta, t->smooth);
         CUDA_TRY(cudaGetLastError());
         dev::StatsArgs ad = a;
         ad.V = std::min(a.V, t->Vd);
         if (ad.V > ad.wlo) {
-            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats, (ad.V - ad.wlo + t->warps - 1) / t->warps));
-            dev::k_word_stats<<<grid, 32 * t->warps, t->smem_stats, t->stream>>>(ad);
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats_dense, (ad.V - ad.wlo + 7) / 8));
+            dev::k_word_stats_dense_rows<<<grid, 256, (size_t)t->K * 4, t->stream>>>(ad);
             CUDA_TRY(cudaGetLastError());
         }
         if (a.V > std::max(t->Vd, a.wlo)) {
@@ -917,8 +930,16 @@ static dev::DtArgs dt_args(const lda_trainer* t, int chunk, int slot) {
 static int launch_dt(const lda_trainer* t, const dev::DtArgs& a, cudaStream_t q) {
     const int64_t nd = a.d_end - a.d_begin;
     if (t->large) {
+        // docs of at most kSmallDoc tokens warp per doc, longer ones CTA per doc
+        dev::DtArgs as = a;
+        as.small_max = t->grid_dt_small > 0 ? (uint32_t)dev::kSmallDoc : 0u;
+        if (as.small_max) {
+            const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt_small, (nd + 7) / 8));
+            dev::k_dt_build_small<<<grid, 256, t->smem_dt_small, q>>>(as);
+            CUDA_TRY(cudaGetLastError());
+        }
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt_cta, nd));
-        dev::k_dt_build_cta<<<grid, dev::kRebuildThreads, t->smem_dt_cta, q>>>(a);
+        dev::k_dt_build_cta<<<grid, dev::kRebuildThreads, t->smem_dt_cta, q>>>(as);
     } else {
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_dt, (nd + t->warps_dt - 1) / t->warps_dt));
         dev::k_dt_build<true><<<grid, 32 * t->warps_dt, t->smem_dt, q>>>(a);
@@ -1801,7 +1822,7 @@ extern "C" int lda_sample_chunk_noalloc(const lda_sample_io* io, int32_t device,
     a.dt_base = 0;
     if (io->K > dev::kLargeK) {
         a.smooth = reinterpret_cast<const float*>(scratch + kNoAllocSmooth);
-        dev::k_smooth_table<<<1, 32, 0, st>>>(io->n_k, io->K, a.Vbeta, io->alpha, io->beta,
+        dev::k_smooth_table<<<1, 1024, 0, st>>>(io->n_k, io->K, a.Vbeta, io->alpha, io->beta,
                                               reinterpret_cast<float*>(scratch + kNoAllocSmooth));
         CUDA_TRY(cudaGetLastError());
     }
