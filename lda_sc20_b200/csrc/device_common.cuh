@@ -6,7 +6,14 @@
 #pragma once
 
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
+
+// The trainer's doc rows up to kLargeK topics hold 8-byte entries {slot key, count as a
+// float} when LDA_ROW8 is set, so that a row-sum step needs no key or count extraction.
+#ifndef LDA_ROW8
+#define LDA_ROW8 0
+#endif
 
 namespace lda {
 namespace dev {
@@ -326,13 +333,16 @@ __host__ __device__ __forceinline__ int col_unskew(int s) { return s - s / 33; }
 // slot already zeroed); SKEWKEYS: the rows' keys are slot indices.
 template <bool SKEWKEYS>
 struct ColSharedT {
+    // a row entry: (key << 16) | count, or with LDA_ROW8 the trainer's {key, count as float}
+    using Entry = typename std::conditional<SKEWKEYS && LDA_ROW8, uint2, uint32_t>::type;
     const float* col;
     __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
     __device__ __forceinline__ float row(uint32_t key) const { return col[SKEWKEYS ? (int)key : col_skew((int)key)]; }
     __device__ __forceinline__ int topic(uint32_t key) const { return SKEWKEYS ? col_unskew((int)key) : (int)key; }
-    // an entry is (key << 16) | count
     __device__ __forceinline__ uint32_t key(uint32_t e) const { return e >> 16; }
     __device__ __forceinline__ float cnt(uint32_t e) const { return u2f(e & 0xffffu); }
+    __device__ __forceinline__ uint32_t key(uint2 e) const { return e.x; }
+    __device__ __forceinline__ float cnt(uint2 e) const { return __uint_as_float(e.y); }
 };
 using ColShared = ColSharedT<false>;
 
@@ -343,13 +353,14 @@ using ColShared = ColSharedT<false>;
 // ROWM 1: the loads of four steps, then of two, then one, are issued before their use
 // (rows that often miss L2, at large K); ROWM 0: two steps at a time.
 template <int ROWM = 0, class View>
-__device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uint32_t lane, uint32_t nnz,
+__device__ __forceinline__ float lane_mass(const typename View::Entry* __restrict__ row, uint32_t lane, uint32_t nnz,
                                            const View& colz, float acc = 0.0f) {
+    using E = typename View::Entry;
     uint32_t q = lane;
     if (ROWM == 1) {
         for (; q + 96u < nnz; q += 128u) {
-        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
-                       e3 = __ldg(row + q + 96u);
+        const E e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
+                e3 = __ldg(row + q + 96u);
         acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
         acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
         acc = ffma(colz.cnt(e2), colz.row(colz.key(e2)), acc);
@@ -358,12 +369,12 @@ __device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uin
     }
     // the loads of two steps issued together
     for (; q + 32u < nnz; q += 64u) {
-        const uint32_t e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
+        const E e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
         acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
         acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
     }
     if (q < nnz) {
-        const uint32_t e = __ldg(row + q);
+        const E e = __ldg(row + q);
         acc = ffma(colz.cnt(e), colz.row(colz.key(e)), acc);
     }
     return acc;
@@ -375,14 +386,15 @@ __device__ __forceinline__ float lane_mass(const uint32_t* __restrict__ row, uin
 // `fallback`.  Each entry of the lane sits on its own 128-byte line, so the loads of four
 // entries are issued before any of them is used.
 template <class View>
-__device__ __forceinline__ int lane_draw(const uint32_t* __restrict__ row, uint32_t ls, uint32_t nnz,
+__device__ __forceinline__ int lane_draw(const typename View::Entry* __restrict__ row, uint32_t ls, uint32_t nnz,
                                          const View& colz, float t2, int fallback) {
+    using E = typename View::Entry;
     float acc = 0.0f;
     int last = -1;
     for (uint32_t q = ls; q < nnz; q += 128u) {
-        uint32_t e[4];
+        E e[4];
 #pragma unroll
-        for (int s = 0; s < 4; ++s) e[s] = q + 32u * s < nnz ? __ldg(row + q + 32u * s) : 0u;
+        for (int s = 0; s < 4; ++s) e[s] = q + 32u * s < nnz ? __ldg(row + q + 32u * s) : E{};
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
             if (q + 32u * s >= nnz) break;

@@ -620,6 +620,7 @@ k_sample_t(SampleArgs a) {
 // the number of set bits before each 32-topic word; a topic's count is read from the
 // word's row (ascending k), and phi_k is formed exactly as build_column forms it.
 struct ColBits {
+    using Entry = uint32_t;  // a doc-row entry: (k << 16) | count
     const uint32_t* bits;  // ceil(K/32) words
     const uint16_t* pre;   // set bits before each word
     const uint32_t* ent;   // the word's row, (k << 16) | count
@@ -862,23 +863,21 @@ __device__ __forceinline__ void top3_insert(float v, int k, float& a1, int& i1, 
     }
 }
 
+// Shared memory of the sparse-word statistics: the order list, then per warp the bitmap.
+// The reciprocals are read from the global table (k_recip), so that the CTA does not
+// hold K of them and eight CTAs fit per SM.
 __host__ __device__ __forceinline__ size_t stats_sparse_smem(int K, int warps) {
-    return (size_t)K * 4 + kOrderList * 4 + (size_t)warps * (large_bit_words(K) * 4);
+    return kOrderList * 4 + (size_t)warps * (large_bit_words(K) * 4);
 }
 
-__global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
-    extern __shared__ float smf[];
+// The first kOrderList topics by (beta * r_k desc, k asc), by repeated CTA-wide arg-max
+// over the global reciprocal table (k_recip); one CTA.
+__global__ void __launch_bounds__(256) k_sparse_order(StatsArgs a, int* order) {
     __shared__ float red_v[8];
     __shared__ int red_k[8];
+    __shared__ int pick;
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int bw = large_bit_words(a.K);
-    float* r = smf;
-    int* order = reinterpret_cast<int*>(smf + a.K);
-    uint32_t* bits = reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * wid;
-    fill_recip(r, a.n_k, a.K, a.Vbeta);
-    for (int i = lane; i < bw; i += 32) bits[i] = 0u;
-    __syncthreads();
-    // the first kOrderList topics by (beta * r_k desc, k asc): repeated CTA-wide arg-max
+    const float* __restrict__ r = a.recip;
     const int L = min(kOrderList, a.K);
     float pv = __int_as_float(0x7f800000);  // the previous pick; the next is the best ranked after it
     int pk = -1;
@@ -898,11 +897,26 @@ __global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
             for (int i = 1; i < warps; ++i)
                 if (ranks_above(red_v[i], red_k[i], v, k)) { v = red_v[i]; k = red_k[i]; }
             order[n] = k;
+            pick = k;
         }
         __syncthreads();
-        pk = order[n];
+        pk = pick;
         pv = fmul(a.beta, r[pk]);
+        __syncthreads();
     }
+}
+
+__global__ void __launch_bounds__(256) k_word_stats_sparse_large(StatsArgs a) {
+    extern __shared__ float smf[];
+    const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bw = large_bit_words(a.K);
+    const float* __restrict__ r = a.recip;
+    int* order = reinterpret_cast<int*>(smf);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(order + kOrderList) + (size_t)bw * wid;
+    const int L = min(kOrderList, a.K);
+    for (int i = threadIdx.x; i < L; i += blockDim.x) order[i] = __ldg(a.order + i);
+    for (int i = lane; i < bw; i += 32) bits[i] = 0u;
+    __syncthreads();
     for (int w = max(a.Vd, a.wlo) + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps) {
         const int s = w - a.Vd;
         const uint32_t* ent = a.swt_ent + __ldg(a.swt_off + s);

@@ -134,6 +134,8 @@ struct StatsArgs {
     float* st_ql;       // [V*32]
     const float* smooth = nullptr;  // K > kLargeK: the smoothing table (k_smooth_table)
     int wlo = 0;                    // the words [wlo, V) get statistics (a word range)
+    const float* recip = nullptr;   // K > kLargeK: r_k as fill_recip forms it (k_recip)
+    const int* order = nullptr;     // K > kLargeK: the sparse words' topic order (k_sparse_order)
 };
 
 // Statistics of word w from its column (built into the warp's shared `col`).
@@ -312,7 +314,12 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& his
             const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
             m &= m - 1u;
             const uint32_t key = a.K <= kLargeK ? (uint32_t)col_skew((int)k) : k;
-            out[p++] = (key << 16) | hist.get(k);
+            if (LDA_ROW8 && a.K <= kLargeK) {
+                reinterpret_cast<uint2*>(a.dt_ent)[(out - a.dt_ent) + p++] =
+                    make_uint2(key, __float_as_uint((float)hist.get(k)));
+            } else {
+                out[p++] = (key << 16) | hist.get(k);
+            }
             hist.clear(k);
         }
     }
@@ -453,8 +460,10 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
     // their ratio per 16 tokens (earlier if a product leaves [1e-150, 1e150])
     double ll_num = 1.0, ll_den = 1.0;
     int ll_n = 0;
+    using E = typename View::Entry;
+    const E* rows = reinterpret_cast<const E*>(a.dt_ent);
     uint32_t cur = 0xffffffffu, nnz = 0;
-    const uint32_t* row = a.dt_ent;
+    const E* row = rows;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
     unsigned spos = 0u;  // lanes of the current row with a positive sum
     for (uint32_t g = g0; g < cnt; g += gstep) {
@@ -493,7 +502,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
             if (dj != cur) {
                 cur = dj;
                 nnz = __shfl_sync(FULL, my_nnz, j);
-                row = a.dt_ent + __shfl_sync(FULL, my_off, j);
+                row = rows + __shfl_sync(FULL, my_off, j);
                 SL = lane_mass<ROWM>(row, (uint32_t)lane, nnz, colz);
                 SP = warp_ks_scan(SL, lane);
                 S = __shfl_sync(FULL, SP, 31);
@@ -561,7 +570,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
             }
         }
         // an S-bucket token's row is its own doc's: the lane holds its offset and length
-        if (kind == BR_S) znew = lane_draw(a.dt_ent + my_off, my_ls, my_nnz, colz, my_t2, maxK);
+        if (kind == BR_S) znew = lane_draw(rows + my_off, my_ls, my_nnz, colz, my_t2, maxK);
         if (valid) a.z[tok] = (uint16_t)znew;
         // counters of the group: ballots and warp sums instead of per-token updates
         const bool in_need = (need0 >> lane) & 1u;
