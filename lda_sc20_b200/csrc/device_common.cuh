@@ -6,14 +6,7 @@
 #pragma once
 
 #include <cstdint>
-#include <type_traits>
 #include <cuda_runtime.h>
-
-// The trainer's doc rows up to kLargeK topics hold 8-byte entries {slot key, count as a
-// float} when LDA_ROW8 is set, so that a row-sum step needs no key or count extraction.
-#ifndef LDA_ROW8
-#define LDA_ROW8 0
-#endif
 
 namespace lda {
 namespace dev {
@@ -333,16 +326,13 @@ __host__ __device__ __forceinline__ int col_unskew(int s) { return s - s / 33; }
 // slot already zeroed); SKEWKEYS: the rows' keys are slot indices.
 template <bool SKEWKEYS>
 struct ColSharedT {
-    // a row entry: (key << 16) | count, or with LDA_ROW8 the trainer's {key, count as float}
-    using Entry = typename std::conditional<SKEWKEYS && LDA_ROW8, uint2, uint32_t>::type;
+    using Entry = uint32_t;  // a doc-row entry: (key << 16) | count
     const float* col;
     __device__ __forceinline__ float operator()(int k) const { return col[col_skew(k)]; }
     __device__ __forceinline__ float row(uint32_t key) const { return col[SKEWKEYS ? (int)key : col_skew((int)key)]; }
     __device__ __forceinline__ int topic(uint32_t key) const { return SKEWKEYS ? col_unskew((int)key) : (int)key; }
     __device__ __forceinline__ uint32_t key(uint32_t e) const { return e >> 16; }
     __device__ __forceinline__ float cnt(uint32_t e) const { return u2f(e & 0xffffu); }
-    __device__ __forceinline__ uint32_t key(uint2 e) const { return e.x; }
-    __device__ __forceinline__ float cnt(uint2 e) const { return __uint_as_float(e.y); }
 };
 using ColShared = ColSharedT<false>;
 

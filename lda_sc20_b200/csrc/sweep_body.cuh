@@ -314,12 +314,7 @@ __device__ __forceinline__ void dt_doc(const DtArgs& a, uint32_t d, const H& his
             const uint32_t k = (uint32_t)wi * 32u + (uint32_t)(__ffs(m) - 1);
             m &= m - 1u;
             const uint32_t key = a.K <= kLargeK ? (uint32_t)col_skew((int)k) : k;
-            if (LDA_ROW8 && a.K <= kLargeK) {
-                reinterpret_cast<uint2*>(a.dt_ent)[(out - a.dt_ent) + p++] =
-                    make_uint2(key, __float_as_uint((float)hist.get(k)));
-            } else {
-                out[p++] = (key << 16) | hist.get(k);
-            }
+            out[p++] = (key << 16) | hist.get(k);
             hist.clear(k);
         }
     }

@@ -323,10 +323,6 @@ static void launch_sample(bool ll, int K, int grid, int threads, size_t smem, cu
     }
 }
 
-// 32-bit words per doc-row entry of the trainer: 2 with 8-byte entries (LDA_ROW8, up to
-// kLargeK topics), else 1
-static int64_t row_words(const lda_trainer& T) { return LDA_ROW8 && !T.large ? 2 : 1; }
-
 extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* cfg, lda_trainer** out) {
     if (!c || !cfg || !out) return fail(LDA_ERR_ARG, "null argument");
     *out = nullptr;
@@ -499,7 +495,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         // the exact bytes of the resident layout (the allocations below, in resident mode)
         auto nb = [](int64_t n, int64_t size) { return std::max<int64_t>(n, 1) * size; };
         const int64_t ns = (int64_t)st.size(), nw = (int64_t)wt.size();
-        const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap * row_words(T), 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
+        const int64_t resident = 4 * nb(N, 4) + nb(T.dt_cap, 4) + nb(N, 2) + nb(D + 1, 4) + 3 * nb(D, 4) +
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
                                  nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(3 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? 2 * nb(T.K, 4) + nb(dev::kOrderList, 4) : 0) +
@@ -509,13 +505,13 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     int rc;
 #define ALLOC(p, n) if ((rc = T.alloc(&(p), (n))) != LDA_OK) return rc
     if (!T.streaming) {
-        ALLOC(T.tok_doc, N); ALLOC(T.meta, N); ALLOC(T.dtok_pos, N); ALLOC(T.dtok_word, N); ALLOC(T.dt_ent, T.dt_cap * row_words(T));
+        ALLOC(T.tok_doc, N); ALLOC(T.meta, N); ALLOC(T.dtok_pos, N); ALLOC(T.dtok_word, N); ALLOC(T.dt_ent, T.dt_cap);
     } else {
         const int ns = cfg->num_streams > 0 ? cfg->num_streams : 4;
         T.slots.resize(ns);
         for (auto& sl : T.slots) {
             ALLOC(sl.tok_doc, T.max_chunk_tok); ALLOC(sl.dtok_pos, T.max_chunk_tok); ALLOC(sl.dtok_word, T.max_chunk_tok);
-            ALLOC(sl.meta, T.max_chunk_tok); ALLOC(sl.dt_ent, T.max_chunk_dt * row_words(T));
+            ALLOC(sl.meta, T.max_chunk_tok); ALLOC(sl.dt_ent, T.max_chunk_dt);
         }
         T.sstreams.resize(ns, nullptr);
         T.ev_slot.resize(ns, nullptr);
@@ -1627,32 +1623,21 @@ extern "C" int64_t lda_get_doc_rows(lda_trainer* t, int64_t* off, uint32_t* ent,
     if (!t || !off) return fail(LDA_ERR_ARG, "null argument");
     CUDA_TRY(cudaSetDevice(t->device));
     CUDA_TRY(cudaStreamSynchronize(t->stream));
-    const int64_t rw = row_words(*t);
-    std::vector<uint32_t> hoff(t->D), hnnz(t->D), hent(std::max<int64_t>(t->dt_cap * rw, 1));
+    std::vector<uint32_t> hoff(t->D), hnnz(t->D), hent(std::max<int64_t>(t->dt_cap, 1));
     CUDA_TRY(cudaMemcpy(hoff.data(), t->dt_off, sizeof(uint32_t) * (size_t)t->D, cudaMemcpyDeviceToHost));
     CUDA_TRY(cudaMemcpy(hnnz.data(), t->dt_nnz, sizeof(uint32_t) * (size_t)t->D, cudaMemcpyDeviceToHost));
-    CUDA_TRY(cudaMemcpy(hent.data(), t->dt_ent, sizeof(uint32_t) * (size_t)(t->dt_cap * rw), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(hent.data(), t->dt_ent, sizeof(uint32_t) * (size_t)t->dt_cap, cudaMemcpyDeviceToHost));
     int64_t n = 0;
     off[0] = 0;
     for (int64_t d = 0; d < t->D; ++d) {
         if (ent) {
             if (n + hnnz[d] > cap) return fail(LDA_ERR_ARG, "doc-row buffer too small");
-            const uint32_t* src = hent.data() + (size_t)hoff[d] * rw;
+            const uint32_t* src = hent.data() + hoff[d];
             for (uint32_t j = 0; j < hnnz[d]; ++j) {
-                // up to kLargeK topics the device rows carry word-column slot indices (with
-                // 8-byte entries: {slot, count as float})
-                uint32_t key, cnt;
-                if (rw == 2) {
-                    key = src[2 * j];
-                    float f;
-                    std::memcpy(&f, &src[2 * j + 1], sizeof f);
-                    cnt = (uint32_t)f;
-                } else {
-                    key = src[j] >> 16;
-                    cnt = src[j] & 0xffffu;
-                }
+                // up to kLargeK topics the device rows carry word-column slot indices
+                const uint32_t key = src[j] >> 16;
                 const uint32_t k = t->K <= dev::kLargeK ? (uint32_t)dev::col_unskew((int)key) : key;
-                ent[n + j] = (k << 16) | cnt;
+                ent[n + j] = (k << 16) | (src[j] & 0xffffu);
             }
         }
         n += hnnz[d];
