@@ -322,3 +322,25 @@ def test_word_and_doc_sharding_on_one_gpu_match_single_trainer(K, over):
         n = sum(x[1] for x in lls)
         fs, fn = full.loglik()
         assert n == fn and abs(s - fs) <= 1e-9 * abs(fs), (it, s, fs)
+
+
+@pytest.mark.gpu
+def test_word_range_guards_whole_sweeps():
+    """With a word range set, the trainer's own whole sweeps would sample from one rank's
+    partial counts, so they are refused (LDA_ERR_STATE); clearing the range (the whole
+    vocabulary) makes them run again.  A range outside the vocabulary is an argument
+    error."""
+    c = L.Corpus.generate(L.corpus_config("c0", num_chunks=2))
+    V = c.info.vocab
+    tr = L.Trainer(c, K=64)
+    tr.set_word_range(0, V // 2)
+    with pytest.raises(L.LdaError) as e:
+        tr.iterate(1)
+    assert e.value.code == -7
+    with pytest.raises(L.LdaError) as e:
+        tr.set_word_range(0, V + 1)
+    assert e.value.code == -1
+    tr.set_word_range(0, V)
+    tr.iterate(1)
+    ws = tr.word_side()
+    assert (ws.K, ws.vocab, ws.num_dense) == (64, V, c.info.num_dense) and ws.n_k and ws.top2
