@@ -753,9 +753,13 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
 }
 
 template <bool LL, int QB>
+#ifndef LDA_DENSE_DYN
+#define LDA_DENSE_DYN 1
+#endif
 __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dense_large(SampleArgs a) {
     extern __shared__ float smf[];
     __shared__ int s_tile;
+    __shared__ uint32_t s_group;  // plain sweeps: the tile's next 32-token group
     const int warps = blockDim.x >> 5, wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float* col = smf;
     uint32_t* ctr_all = reinterpret_cast<uint32_t*>(col + col_words(a.K));
@@ -785,6 +789,7 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
         if (threadIdx.x == 0) {
             col[col_skew(maxK)] = 0.0f;
             ctr[C_TDENSE] += 1u;
+            s_group = 0u;
         }
         __syncthreads();
         if (qr) {
@@ -822,7 +827,8 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
         const float Q = __shfl_sync(FULL, QP, 31);
         double ll = sample_groups<LL, QB, false, LDA_LARGE_ROW_MODE>(a, (uint32_t)t.y, (uint32_t)t.z, 32u * wid,
                                                                      32u * warps, a.iter, maxK, ph, QL, QP, Q,
-                                                                     ColShared{col}, ctr, lane, qr ? qtab : nullptr, qr);
+                                                                     ColShared{col}, ctr, lane, qr ? qtab : nullptr, qr,
+                                                                     nullptr, (!LL && LDA_DENSE_DYN) ? &s_group : nullptr);
         if (LL) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);

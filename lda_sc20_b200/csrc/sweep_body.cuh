@@ -442,14 +442,21 @@ constexpr int kSampleWarps = LDA_SAMPLE_WARPS;
 #endif
 
 // The 32-token groups g0, g0 + gstep, ... of the token range [start, start + cnt) of one
-// word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word).
-// Returns the lane's LL partial (LL mode).
+// word (column view colz, max topic maxK, phi4 ph, Q partials QL / QP / Q of the word), or,
+// with a shared group counter gq, the groups the warp claims from it (32 tokens at a time,
+// so that the warps sharing a tile finish it together).  Returns the lane's LL partial (LL
+// mode).
 template <bool LL, int QB, bool SPLIT = false, int ROWM = 0, class View>
 __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t start, uint32_t cnt, uint32_t g0,
                                                 uint32_t gstep, uint32_t iter, int maxK, const float4 ph, float QL,
                                                 float QP, float Q, const View& colz, uint32_t* ctr, int lane,
                                                 const float2* qtab = nullptr, int qrounds = 0,
-                                                const SplitQ* sq = nullptr) {
+                                                const SplitQ* sq = nullptr, uint32_t* gq = nullptr) {
+    auto claim = [&]() {
+        uint32_t v = 0;
+        if (lane == 0) v = atomicAdd(gq, 32u);
+        return __shfl_sync(FULL, v, 0);
+    };
     double ll = 0.0;
     // LL mode: the lane's factors total_t and (n_d + K alpha) as FP64 products, one log of
     // their ratio per 16 tokens (earlier if a product leaves [1e-150, 1e150])
@@ -461,7 +468,7 @@ __device__ __forceinline__ double sample_groups(const SampleArgs& a, uint32_t st
     const E* row = rows;
     float SL = 0.0f, SP = 0.0f, S = 0.0f;
     unsigned spos = 0u;  // lanes of the current row with a positive sum
-    for (uint32_t g = g0; g < cnt; g += gstep) {
+    for (uint32_t g = gq ? claim() : g0; g < cnt; g = gq ? claim() : g + gstep) {
         const bool valid = g + lane < cnt;
         const uint32_t tok = start + g + lane;
         uint32_t d = 0xffffffffu, nd = 0, my_nnz = 0, my_off = 0;
