@@ -677,6 +677,11 @@ __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
 #define LDA_LARGE_ROW_MODE 1
 #endif
 
+// The sparse-word sampler keeps each word's Qw rounds' table in registers (lane r: round
+// r), so a Q draw evaluates the one round that holds its target instead of walking them.
+#ifndef LDA_QW_TABLE
+#define LDA_QW_TABLE 1
+#endif
 template <bool LL, int QB>
 __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_sparse_large(SampleArgs a) {
     extern __shared__ float smf[];
@@ -735,7 +740,12 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         const float Q = __shfl_sync(FULL, QP, 31);
         __syncwarp();
         const ColBits view{bits, pre, ent, r, a.beta, maxK};
+#if LDA_QW_TABLE
+        SplitQ sq{ent, nnz_w, __shfl_sync(FULL, QL, 0), a.smooth, r, true};
+        split_q_table(sq, maxK, a.alpha, lane);
+#else
         const SplitQ sq{ent, nnz_w, __shfl_sync(FULL, QL, 0), a.smooth, r, true};
+#endif
         double ll = sample_groups<LL, QB, true, LDA_LARGE_ROW_MODE>(a, (uint32_t)t.y, (uint32_t)t.z, 0u, 32u, a.iter,
                                                                     maxK, ph, QL, QP, Q, view, ctr, lane, nullptr, 0,
                                                                     &sq);

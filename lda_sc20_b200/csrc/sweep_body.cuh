@@ -383,8 +383,47 @@ struct SplitQ {
     const float* T;       // the smoothing table (K entries, non-decreasing)
     const float* r;       // r_k, at col_skew(k) when skew
     bool skew;
+    // the Qw rounds' table, lane r holding round r's (carry before it, carry + its largest
+    // KS prefix); rounds = 0 when not built (more than 32 rounds, or not wanted)
+    int rounds = 0;
+    float qcarry = 0.0f, qthr = 0.0f;
     __device__ __forceinline__ float rk(int k) const { return r[skew ? col_skew(k) : k]; }
+    // round slot i of the Qw search: alpha * (n_wk * r_k), the max topic's term 0
+    __device__ __forceinline__ void slot(uint32_t i, int maxK, float alpha, int& key, float& term, bool& ok) const {
+        const uint32_t en = __ldg(ent + i);
+        const int k = (int)(en >> 16);
+        term = k == maxK ? 0.0f : fmul(alpha, fmul(u2f(en & 0xffffu), rk(k)));
+        key = k;
+        ok = term > 0.0f;
+    }
 };
+
+// Builds the Qw rounds' table of a split word (at most 32 rounds of 32 entries): each
+// round's total and largest lane prefix from its Kogge-Stone scan, and the carries as the
+// fadd chain of the totals, the values warp_level2 forms round by round.  Warp-uniform.
+__device__ __forceinline__ void split_q_table(SplitQ& q, int maxK, float alpha, int lane) {
+    const uint32_t R = (q.nnz + 31u) >> 5;
+    if (R == 0 || R > 32) return;
+    float carry = 0.0f;
+    for (uint32_t r = 0; r < R; ++r) {
+        int key = -1;
+        float term = 0.0f;
+        bool ok = false;
+        const uint32_t i = 32u * r + (uint32_t)lane;
+        if (i < q.nnz) q.slot(i, maxK, alpha, key, term, ok);
+        const float ks = warp_ks_scan(term, lane);
+        float mx = ks;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_xor_sync(FULL, mx, off));
+        const float tot = __shfl_sync(FULL, ks, 31);
+        if ((uint32_t)lane == r) {
+            q.qcarry = carry;
+            q.qthr = fadd(carry, mx);
+        }
+        carry = fadd(carry, tot);
+    }
+    q.rounds = (int)R;
+}
 
 // The Q-bucket draw of a split word for t = target - pS (uniform across the warp): the
 // word's own topics first, in rounds of 32 entries (carry + Kogge-Stone scan of
@@ -395,14 +434,27 @@ struct SplitQ {
 __device__ __forceinline__ int split_q_draw(const SplitQ& q, float t, int maxK, int K, float alpha, float beta,
                                             int lane) {
     if (t < q.Qw) {
-        auto slot = [&](uint32_t i, int& key, float& term, bool& ok) {
-            const uint32_t en = __ldg(q.ent + i);
-            const int k = (int)(en >> 16);
-            term = k == maxK ? 0.0f : fmul(alpha, fmul(u2f(en & 0xffffu), q.rk(k)));
-            key = k;
-            ok = term > 0.0f;
-        };
-        const int z = warp_level2(q.nnz, t, -1, lane, slot);
+        auto slot = [&](uint32_t i, int& key, float& term, bool& ok) { q.slot(i, maxK, alpha, key, term, ok); };
+        int z = -1;
+        if (q.rounds > 0) {
+            // the candidate rounds (t below the round's largest prefix), in order
+            for (unsigned b = __ballot_sync(FULL, lane < q.rounds && t < q.qthr); b; b &= b - 1u) {
+                const uint32_t r = (uint32_t)(__ffs(b) - 1);
+                const float carry = __shfl_sync(FULL, q.qcarry, (int)r);
+                int key = -1;
+                float term = 0.0f;
+                bool ok = false;
+                const uint32_t i = 32u * r + (uint32_t)lane;
+                if (i < q.nnz) slot(i, key, term, ok);
+                const float ks = warp_ks_scan(term, lane);
+                const unsigned f = __ballot_sync(FULL, ok && t < fadd(carry, ks));
+                if (f) {
+                    z = __shfl_sync(FULL, key, __ffs(f) - 1);
+                    break;
+                }
+            }
+        }
+        if (z < 0) z = warp_level2(q.nnz, t, -1, lane, slot);
         if (z >= 0) return z;
     }
     const float t1 = fsub(t, q.Qw);

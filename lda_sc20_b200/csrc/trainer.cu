@@ -25,7 +25,7 @@ using namespace lda;
 namespace {
 
 #ifndef LDA_SAMPLE_TILE
-#define LDA_SAMPLE_TILE 512
+#define LDA_SAMPLE_TILE 1024
 #endif
 constexpr int kSampleTile = LDA_SAMPLE_TILE;  // most tokens per sampler tile (a word's column is rebuilt per tile)
 constexpr int kSampleTileMin = 64;            // fewest tokens per tile that a chunk's tile size goes down to
