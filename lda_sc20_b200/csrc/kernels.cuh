@@ -711,24 +711,15 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         const int s = w - a.Vd;
         const uint32_t* ent = a.swt_ent + __ldg(a.swt_off + s);
         const uint32_t nnz_w = __ldg(a.swt_nnz + s);
+        // the word's topics into the bitmap; pre[j] = the rank of the first of the word's
+        // topics in bitmap word j (the entries ascend, so that is the entry's index).  Only
+        // words with a set bit are ever read, so the others are left as they are.
         for (uint32_t e = lane; e < nnz_w; e += 32) {
             const uint32_t k = __ldg(ent + e) >> 16;
             atomicOr(&bits[k >> 5], 1u << (k & 31u));
+            if (e == 0 || (__ldg(ent + e - 1) >> 21) != (k >> 5)) pre[k >> 5] = (uint16_t)e;
         }
         __syncwarp();
-        uint32_t carry = 0;
-        for (int wb = 0; wb < bw; wb += 32) {
-            const int i = wb + lane;
-            const uint32_t c = i < bw ? (uint32_t)__popc(bits[i]) : 0u;
-            uint32_t incl = c;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const uint32_t v = __shfl_up_sync(FULL, incl, off);
-                if (lane >= off) incl += v;
-            }
-            if (i < bw) pre[i] = (uint16_t)(carry + incl - c);
-            carry += __shfl_sync(FULL, incl, 31);
-        }
         if (lane == 0) {
             ctr[C_WNNZ] += nnz_w;
             ctr[C_TSPARSE] += 1u;

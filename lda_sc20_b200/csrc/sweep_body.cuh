@@ -398,12 +398,12 @@ struct SplitQ {
     }
 };
 
-// Builds the Qw rounds' table of a split word (at most 32 rounds of 32 entries): each
+// Builds the Qw rounds' table of a split word (2 to 32 rounds of 32 entries): each
 // round's total and largest lane prefix from its Kogge-Stone scan, and the carries as the
 // fadd chain of the totals, the values warp_level2 forms round by round.  Warp-uniform.
 __device__ __forceinline__ void split_q_table(SplitQ& q, int maxK, float alpha, int lane) {
     const uint32_t R = (q.nnz + 31u) >> 5;
-    if (R == 0 || R > 32) return;
+    if (R < 2 || R > 32) return;  // one round: the walk is that round already
     float carry = 0.0f;
     for (uint32_t r = 0; r < R; ++r) {
         int key = -1;
