@@ -677,6 +677,9 @@ __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
 #define LDA_LARGE_ROW_MODE 1
 #endif
 
+#ifndef LDA_CLAIM_AHEAD
+#define LDA_CLAIM_AHEAD 1
+#endif
 // The sparse-word sampler keeps each word's Qw rounds' table in registers (lane r: round
 // r), so a Q draw evaluates the one round that holds its target instead of walking them.
 #ifndef LDA_QW_TABLE
@@ -701,16 +704,24 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
     for (int i = lane; i < bw; i += 32) bits[i] = 0u;
     if (lane < C_NUM) ctr[lane] = 0u;
     __syncthreads();
+    // the next tile is claimed when a tile starts, so that the claim's round trip overlaps
+    // the tile's work
+    int tile = 0;
+    if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(FULL, tile, 0);
     for (;;) {
-        int tile = 0;
-        if (lane == 0) tile = (int)atomicAdd(a.tile_counter, 1u);
-        tile = __shfl_sync(FULL, tile, 0);
         if (tile >= a.ntiles) break;
+        int next = 0;
+        if (LDA_CLAIM_AHEAD && lane == 0) next = (int)atomicAdd(a.tile_counter, 1u);
         const int4 t = a.tiles[tile];
         const int w = t.x;
         const int s = w - a.Vd;
         const uint32_t* ent = a.swt_ent + __ldg(a.swt_off + s);
         const uint32_t nnz_w = __ldg(a.swt_nnz + s);
+        // the word's statistics, loaded before the bitmap work so that their loads overlap it
+        const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
+        const float4 ph = __ldg(a.st_phi + w);
+        const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
         // the word's topics into the bitmap; pre[j] = the rank of the first of the word's
         // topics in bitmap word j (the entries ascend, so that is the entry's index).  Only
         // words with a set bit are ever read, so the others are left as they are.
@@ -724,9 +735,6 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
             ctr[C_WNNZ] += nnz_w;
             ctr[C_TSPARSE] += 1u;
         }
-        const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
-        const float4 ph = __ldg(a.st_phi + w);
-        const float QL = __ldg(a.st_ql + (size_t)w * 32 + lane);
         const float QP = warp_ks_scan(QL, lane);
         const float Q = __shfl_sync(FULL, QP, 31);
         __syncwarp();
@@ -748,6 +756,8 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         __syncwarp();
         for (uint32_t e = lane; e < nnz_w; e += 32) bits[(__ldg(ent + e) >> 16) >> 5] = 0u;
         __syncwarp();
+        if (!LDA_CLAIM_AHEAD && lane == 0) next = (int)atomicAdd(a.tile_counter, 1u);
+        tile = __shfl_sync(FULL, next, 0);
     }
     __syncwarp();
     if (lane < C_NUM && ctr[lane]) atomicAdd(a.ctr + lane, (unsigned long long)ctr[lane]);
