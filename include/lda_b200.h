@@ -196,7 +196,7 @@ int lda_trainer_set_word_range(lda_trainer* t, int32_t w0, int32_t w1);
  * have dense rows (dense_wt, K int32 each); word num_dense + s has the sparse row
  * sparse_ent[sparse_off[s] .. sparse_off[s] + sparse_nnz[s]) inside a fixed slot that ends
  * at sparse_off[s + 1] (sparse_capacity for the last word).  Per word: top2 and k3
- * (uint32), phi4 (4 floats), ql (32 floats). */
+ * (uint32), phi4 (4 floats), ql (32 floats); per dense word its Q-round table. */
 typedef struct lda_word_side {
     int32_t* n_k;
     int32_t* dense_wt;
@@ -207,7 +207,10 @@ typedef struct lda_word_side {
     uint32_t* k3;
     float* phi4;
     float* ql;
-    int64_t K, vocab, num_dense, sparse_capacity;
+    /* above 2048 topics: each dense word's Q-round table (32 * qtab_rounds pairs of floats),
+     * built with its statistics; NULL (and qtab_rounds 0) otherwise */
+    float* qtab;
+    int64_t K, vocab, num_dense, sparse_capacity, qtab_rounds;
 } lda_word_side;
 int lda_trainer_word_side(lda_trainer* t, lda_word_side* out);
 /* One sweep without its word side: the caller has run lda_update_wt and lda_max_topic (and

@@ -87,7 +87,9 @@ class WordSide(C.Structure):
     _fields_ = [
         ("n_k", C.c_void_p), ("dense_wt", C.c_void_p), ("sparse_ent", C.c_void_p), ("sparse_nnz", C.c_void_p),
         ("sparse_off", C.c_void_p), ("top2", C.c_void_p), ("k3", C.c_void_p), ("phi4", C.c_void_p), ("ql", C.c_void_p),
+        ("qtab", C.c_void_p),
         ("K", C.c_int64), ("vocab", C.c_int64), ("num_dense", C.c_int64), ("sparse_capacity", C.c_int64),
+        ("qtab_rounds", C.c_int64),
     ]
 
 

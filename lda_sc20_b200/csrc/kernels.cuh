@@ -562,7 +562,11 @@ __global__ void __launch_bounds__(256) k_word_stats_dense_rows(StatsArgs a) {
     fill_recip(r, a.n_k, a.K, a.Vbeta);
     __syncthreads();
     for (int w = a.wlo + blockIdx.x * warps + wid; w < a.V; w += gridDim.x * warps)
-        word_stats_from(a, w, DenseRowPhi{a.dwt + (size_t)w * a.K, r, a.beta}, lane);
+    {
+        const DenseRowPhi phi{a.dwt + (size_t)w * a.K, r, a.beta};
+        const int k1 = word_stats_from(a, w, phi, lane);
+        if (a.qtab) word_qtab(a, w, k1, phi, lane);
+    }
 }
 
 // Doc-topic rebuild: warp per doc of one chunk.  P16: 16-bit histogram counts (a doc has
@@ -803,7 +807,12 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
             s_group = 0u;
         }
         __syncthreads();
-        if (qr) {
+        if (qr && a.qtab_g) {
+            // the word's Q-round table, built by the word statistics
+            const float2* src = a.qtab_g + (size_t)w * 32 * qr;
+            for (int i = threadIdx.x; i < 32 * qr; i += blockDim.x) qtab[i] = __ldg(src + i);
+            __syncthreads();
+        } else if (qr) {
             // the Q-round table of this word: for lane slot ls and round r, the KS total and the
             // largest KS prefix of alpha * colz(ls + 32 * (32 r + l)), l = 0..31 (slots past the
             // lane's last topic add 0), the terms and scan of warp_level2_rounds

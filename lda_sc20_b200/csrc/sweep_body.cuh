@@ -136,6 +136,10 @@ struct StatsArgs {
     int wlo = 0;                    // the words [wlo, V) get statistics (a word range)
     const float* recip = nullptr;   // K > kLargeK: r_k as fill_recip forms it (k_recip)
     const int* order = nullptr;     // K > kLargeK: the sparse words' topic order (k_sparse_order)
+    // K > kLargeK: the dense words' Q-round tables (32 lane slots x qrounds float2 per word,
+    // the table k_sample_dense_large would build per tile), or null
+    float2* qtab = nullptr;
+    int qrounds = 0;
 };
 
 // Statistics of word w from its column (built into the warp's shared `col`).
@@ -156,7 +160,7 @@ struct ColumnPhi {
 // The statistics of word w from phi(k), k < K: top three, the lane partials of Q (the
 // max topic excluded) and Q.
 template <class Phi>
-__device__ __forceinline__ void word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane);
+__device__ __forceinline__ int word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane);
 
 __device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const float* r, float* col, int lane) {
     build_column(col, r, w, a.Vd, a.K, a.beta, a.dwt, a.swt_off, a.swt_nnz, a.swt_ent, lane, nullptr);
@@ -164,7 +168,7 @@ __device__ __forceinline__ void word_stats_word(const StatsArgs& a, int w, const
 }
 
 template <class Phi>
-__device__ __forceinline__ void word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane) {
+__device__ __forceinline__ int word_stats_from(const StatsArgs& a, int w, const Phi& phi, int lane) {
     // the lane's top three by (phi desc, k asc) in one pass (k ascends, so a strictly larger
     // value is needed to displace), then three warp-wide pops of the lanes' heads
     float a1 = -1.0f, a2 = -1.0f, a3 = -1.0f;
@@ -210,6 +214,44 @@ __device__ __forceinline__ void word_stats_from(const StatsArgs& a, int w, const
         a.st_phi[w] = make_float4(v1, v2, v3, Q);
     }
     __syncwarp();
+    return k1;
+}
+
+// The Q-round table of dense word w (max topic k1) into a.qtab: for lane slot ls and round
+// r, the Kogge-Stone total and largest prefix of alpha * colz(ls + 32 * (32 r + l)),
+// l = 0..31 (slots past the lane slot's last topic add 0, colz the column with its max
+// topic zeroed), then per lane slot the carries as the fadd chain of the totals: entry
+// (ls, r) = (carry before round r, carry + the round's largest prefix).  The values
+// k_sample_dense_large forms from its shared column with warp scans; here lane ls scans
+// its own slot's 32 terms of a round serially in the same Kogge-Stone order (element l
+// adds element l - off at each step off = 1, 2, ..., 16), so that a round's loads read
+// 1,024 consecutive topics.
+template <class Phi>
+__device__ __forceinline__ void word_qtab(const StatsArgs& a, int w, int k1, const Phi& phi, int lane) {
+    const int R = a.qrounds;
+    float2* tab = a.qtab + (size_t)w * 32 * R;
+    const int ls = lane;
+    const uint32_t n = (uint32_t)((a.K - ls + 31) / 32);
+    float carry = 0.0f;
+    for (int r = 0; r < R; ++r) {
+        float v[32];
+#pragma unroll
+        for (int l = 0; l < 32; ++l) {
+            const uint32_t i = 32u * (uint32_t)r + (uint32_t)l;
+            const int k = ls + 32 * (int)i;
+            v[l] = i < n ? fmul(a.alpha, k == k1 ? 0.0f : phi(k)) : 0.0f;
+        }
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int l = 31; l >= off; --l) v[l] = fadd(v[l], v[l - off]);
+        }
+        float mx = v[0];
+#pragma unroll
+        for (int l = 1; l < 32; ++l) mx = fmaxf(mx, v[l]);
+        tab[ls * R + r] = make_float2(carry, fadd(carry, mx));
+        carry = fadd(carry, v[31]);
+    }
 }
 
 // ---------------------------------------------------------------- DT rebuild
@@ -372,6 +414,8 @@ struct SampleArgs {
     const float* recip = nullptr;
     // K > kLargeK: the smoothing table of the split Q bucket (k_smooth_table)
     const float* smooth = nullptr;
+    // K > kLargeK: the dense words' Q-round tables (word_qtab), or null
+    const float2* qtab_g = nullptr;
 };
 
 // The split Q bucket of a sparse word above kLargeK topics: Q = Qw + Qs, Qw over the word's

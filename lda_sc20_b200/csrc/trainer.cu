@@ -58,6 +58,10 @@ struct lda_trainer {
     float* recip = nullptr;  // [K] per-sweep reciprocals (K > kLargeK)
     float* smooth = nullptr; // [K] per-sweep smoothing table of the split Q bucket (K > kLargeK)
     int* order = nullptr;    // [dev::kOrderList] per-sweep topic order of the sparse-word statistics (K > kLargeK)
+    // K > kLargeK: the dense words' Q-round tables, [Vd][32 * qrounds] float2, built by the
+    // word statistics and read by the dense-word sampler (null when dev::qtab_rounds(K) = 0)
+    float2* qtab_g = nullptr;
+    int qrounds = 0;
     int warps_wt = 8, warps_dt = 8;  // warps per CTA of the word-topic and doc-topic rebuilds
     float alpha = 0, beta = 0, Vbeta = 0;
     uint64_t seed = 0;
@@ -499,6 +503,7 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
                                  nb((int64_t)T.Vd * T.K, 4) + 2 * nb(std::max<int64_t>(Vs, 1), 4) + nb(T.swt_cap, 4) +
                                  nb(T.K, 4) + 2 * nb(V, 4) + nb(V, 16) + nb(V * 32, 4) + 2 * nb((int64_t)T.C * V, 4) +
                                  nb(ns, 16) + nb(nw, 16) + nb(ns, 8) + nb(1, 8) + nb(3 + 2 * T.C, 4) + nb(kCounters, 8) + (T.large ? 2 * nb(T.K, 4) + nb(dev::kOrderList, 4) : 0) +
+                                 (T.large && dev::qtab_rounds(T.K) > 0 && T.Vd > 0 ? nb((int64_t)T.Vd * 32 * dev::qtab_rounds(T.K), 8) : 0) +
                                  nb(1, 4);
         T.streaming = cfg->stream_mode == 2 || (cfg->stream_mode == 0 && T.budget > 0 && resident > T.budget);
     }
@@ -544,6 +549,10 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
     ALLOC(T.tile_ll, (int64_t)st.size()); ALLOC(T.ll_dev, 1);
     ALLOC(T.tile_ctr, 3 + 2 * T.C); ALLOC(T.ctr, kCounters); ALLOC(T.err, 1);
     if (T.large) { ALLOC(T.recip, T.K); ALLOC(T.smooth, T.K); ALLOC(T.order, dev::kOrderList); }
+    if (T.large && dev::qtab_rounds(T.K) > 0 && T.Vd > 0) {
+        T.qrounds = dev::qtab_rounds(T.K);
+        ALLOC(T.qtab_g, (int64_t)T.Vd * 32 * T.qrounds);
+    }
 #undef ALLOC
     CUDA_TRY(cudaMallocHost(&T.ll_host, sizeof(double)));
 
@@ -729,6 +738,8 @@ extern "C" int lda_trainer_word_side(lda_trainer* t, lda_word_side* out) {
     out->k3 = t->st_k3;
     out->phi4 = reinterpret_cast<float*>(t->st_phi);
     out->ql = t->st_ql;
+    out->qtab = reinterpret_cast<float*>(t->qtab_g);
+    out->qtab_rounds = t->qrounds;
     out->K = t->K;
     out->vocab = t->V;
     out->num_dense = t->Vd;
@@ -859,6 +870,8 @@ extern "C" int lda_max_topic(lda_trainer* t) {
         CUDA_TRY(cudaGetLastError());
         dev::StatsArgs ad = a;
         ad.V = std::min(a.V, t->Vd);
+        ad.qtab = t->qtab_g;
+        ad.qrounds = t->qrounds;
         if (ad.V > ad.wlo) {
             const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(t->grid_stats_dense, (ad.V - ad.wlo + 7) / 8));
             dev::k_word_stats_dense_rows<<<grid, 256, (size_t)t->K * 4, t->stream>>>(ad);
@@ -973,6 +986,7 @@ static dev::SampleArgs sample_args(const lda_trainer* t, int chunk, int slot, in
     a.tok_doc = b.tok_doc; a.meta = b.meta; a.z = t->z; a.doc_len = t->doc_len;
     a.dt_off = t->dt_off; a.dt_nnz = t->dt_nnz; a.dt_ent = b.dt_ent; a.ctr = t->ctr;
     a.smooth = t->smooth;
+    a.qtab_g = t->qtab_g;
     a.tok_base = b.tok_base;
     a.dt_base = b.dt_base;
     a.recip = t->recip;

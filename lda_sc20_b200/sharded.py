@@ -46,17 +46,18 @@ REBUILD_S_PER_TOKEN = 9.0e-12
 LINK_BYTES_PER_S = 770e9
 
 
-def word_bytes(num_words: int, num_dense: int, K: int, sparse_slot: np.ndarray) -> np.ndarray:
-    """Bytes each word adds to the word-side all-gather: its dense row (4K) or its sparse
-    slot plus row length (4 per entry, 4), and its statistics."""
+def word_bytes(num_words: int, num_dense: int, K: int, sparse_slot: np.ndarray, qtab_rounds: int = 0) -> np.ndarray:
+    """Bytes each word adds to the word-side all-gather: its dense row (4K, plus its Q-round
+    table of 32 x qtab_rounds float pairs) or its sparse slot plus row length (4 per entry,
+    4), and its statistics."""
     b = np.empty(num_words, dtype=np.float64)
-    b[:num_dense] = 4 * K
+    b[:num_dense] = 4 * K + 256 * qtab_rounds
     b[num_dense:] = 4 * (np.asarray(sparse_slot, dtype=np.float64) + 1)
     return b + WORD_STAT_BYTES
 
 
 def word_ranges(word_tokens: np.ndarray, num_dense: int, K: int, sparse_slot: np.ndarray, world: int,
-                s_per_token: float = REBUILD_S_PER_TOKEN, link_bps: float = LINK_BYTES_PER_S):
+                s_per_token: float = REBUILD_S_PER_TOKEN, link_bps: float = LINK_BYTES_PER_S, qtab_rounds: int = 0):
     """Contiguous word ranges, one per rank, for the word side.  A rank's word-side time is
     modelled as its rebuild (tokens x s_per_token) plus the all-gather, whose segments
     are all as large as the largest range's bytes ((world - 1) segments received at
@@ -64,7 +65,7 @@ def word_ranges(word_tokens: np.ndarray, num_dense: int, K: int, sparse_slot: np
     split with the smallest modelled max(rebuild) + all-gather is returned, with that time
     in seconds."""
     tok = np.asarray(word_tokens, dtype=np.float64)
-    byt = word_bytes(len(tok), num_dense, K, sparse_slot)
+    byt = word_bytes(len(tok), num_dense, K, sparse_slot, qtab_rounds)
     ct = np.concatenate([[0.0], np.cumsum(tok)])
     cb = np.concatenate([[0.0], np.cumsum(byt)])
     best, best_t = None, np.inf
@@ -123,14 +124,15 @@ class WordExchange:
     dict of flat byte tensors (the trainer's device arrays, or CPU tensors with gloo):
     "dense" (K int32 per dense word), "sparse_ent" (fixed slots, sparse_off[s] the first
     entry of sparse word s), "sparse_nnz", "top2", "k3", "phi4", "ql", plus the int32
-    "n_k".  A rank's range is a handful of contiguous byte pieces; they are packed into an
+    "n_k", and above 2048 topics "qtab" (each dense word's Q-round table, qtab_bytes per
+    dense word).  A rank's range is a handful of contiguous byte pieces; they are packed into an
     equal-sized send segment (padded to the largest range's, 16-byte aligned), one
     all-gather brings every segment, and the other ranks' pieces are copied into place."""
 
-    FIELDS = ("dense", "sparse_ent", "sparse_nnz", "top2", "k3", "phi4", "ql")
+    FIELDS = ("dense", "sparse_ent", "sparse_nnz", "top2", "k3", "phi4", "ql", "qtab")
     PER_WORD = {"top2": 4, "k3": 4, "phi4": 16, "ql": 128}
 
-    def __init__(self, side, K: int, num_dense: int, sparse_off: np.ndarray, ranges, group=None):
+    def __init__(self, side, K: int, num_dense: int, sparse_off: np.ndarray, ranges, group=None, qtab_bytes: int = 0):
         import torch
         import torch.distributed as dist
         self.side, self.ranges, self.group = side, ranges, group
@@ -145,7 +147,8 @@ class WordExchange:
             s0, s1 = max(w0, num_dense) - num_dense, max(w1, num_dense) - num_dense
             p = [("dense", 4 * K * d0, 4 * K * (d1 - d0)),
                  ("sparse_ent", 4 * int(off[s0]), 4 * int(off[s1] - off[s0])),
-                 ("sparse_nnz", 4 * s0, 4 * (s1 - s0))]
+                 ("sparse_nnz", 4 * s0, 4 * (s1 - s0)),
+                 ("qtab", qtab_bytes * d0, qtab_bytes * (d1 - d0))]
             p += [(f, b * w0, b * (w1 - w0)) for f, b in self.PER_WORD.items()]
             self.pieces.append([x for x in p if x[2] > 0])
         self.seg = max(16, max(sum(n for _, _, n in p) for p in self.pieces))
@@ -226,7 +229,7 @@ def word_side_tensors(trainer, device: int):
     side = {"n_k": view(ws.n_k, K, "<i4"), "dense": view(ws.dense_wt, 4 * K * Vd),
             "sparse_ent": view(ws.sparse_ent, 4 * ws.sparse_capacity), "sparse_nnz": view(ws.sparse_nnz, 4 * (V - Vd)),
             "top2": view(ws.top2, 4 * V), "k3": view(ws.k3, 4 * V), "phi4": view(ws.phi4, 16 * V),
-            "ql": view(ws.ql, 128 * V)}
+            "ql": view(ws.ql, 128 * V), "qtab": view(ws.qtab, 256 * ws.qtab_rounds * Vd)}
     return side, off
 
 
@@ -247,9 +250,10 @@ class ShardedTrainer:
         self.ex = TopicExchange(self.z, self.chunk_tok, self.ranges, group)
         side, off = word_side_tensors(self.tr, device)
         ws = self.tr.word_side()
-        self.word_ranges, self.word_side_s = word_ranges(corpus.word_count(), ws.num_dense, K, np.diff(off), world)
+        self.word_ranges, self.word_side_s = word_ranges(corpus.word_count(), ws.num_dense, K, np.diff(off), world,
+                                                         qtab_rounds=ws.qtab_rounds)
         self.tr.set_word_range(*self.word_ranges[rank])
-        self.wx = WordExchange(side, K, ws.num_dense, off, self.word_ranges, group)
+        self.wx = WordExchange(side, K, ws.num_dense, off, self.word_ranges, group, qtab_bytes=256 * ws.qtab_rounds)
         self.group = group
         self.device = device
 

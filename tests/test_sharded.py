@@ -273,7 +273,9 @@ def test_word_and_doc_sharding_on_one_gpu_match_single_trainer(K, over):
     off = sides[0][1]
     wr, _ = word_ranges(c.word_count(), Vd, K, np.diff(off), 2)
     assert 0 < wr[0][1] < c.info.vocab
-    exs = [WordExchange(s, K, Vd, off, wr) for s, _ in sides]
+    qb = 256 * shards[0].word_side().qtab_rounds
+    assert (qb > 0) == (K > 2048)
+    exs = [WordExchange(s, K, Vd, off, wr, qtab_bytes=qb) for s, _ in sides]
     for t, (a, b), w in zip(shards, ranges, wr):
         t.set_chunk_range(a, b)
         t.set_word_range(*w)
