@@ -681,14 +681,8 @@ __host__ __device__ __forceinline__ size_t dense_large_smem(int K, int warps) {
 #define LDA_LARGE_ROW_MODE 1
 #endif
 
-#ifndef LDA_CLAIM_AHEAD
-#define LDA_CLAIM_AHEAD 1
-#endif
 // The sparse-word sampler keeps each word's Qw rounds' table in registers (lane r: round
 // r), so a Q draw evaluates the one round that holds its target instead of walking them.
-#ifndef LDA_QW_TABLE
-#define LDA_QW_TABLE 1
-#endif
 template <bool LL, int QB>
 __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_sparse_large(SampleArgs a) {
     extern __shared__ float smf[];
@@ -716,7 +710,7 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
     for (;;) {
         if (tile >= a.ntiles) break;
         int next = 0;
-        if (LDA_CLAIM_AHEAD && lane == 0) next = (int)atomicAdd(a.tile_counter, 1u);
+        if (lane == 0) next = (int)atomicAdd(a.tile_counter, 1u);
         const int4 t = a.tiles[tile];
         const int w = t.x;
         const int s = w - a.Vd;
@@ -743,12 +737,8 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         const float Q = __shfl_sync(FULL, QP, 31);
         __syncwarp();
         const ColBits view{bits, pre, ent, r, a.beta, maxK};
-#if LDA_QW_TABLE
         SplitQ sq{ent, nnz_w, __shfl_sync(FULL, QL, 0), a.smooth, r, true};
         split_q_table(sq, maxK, a.alpha, lane);
-#else
-        const SplitQ sq{ent, nnz_w, __shfl_sync(FULL, QL, 0), a.smooth, r, true};
-#endif
         double ll = sample_groups<LL, QB, true, LDA_LARGE_ROW_MODE>(a, (uint32_t)t.y, (uint32_t)t.z, 0u, 32u, a.iter,
                                                                     maxK, ph, QL, QP, Q, view, ctr, lane, nullptr, 0,
                                                                     &sq);
@@ -760,7 +750,6 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
         __syncwarp();
         for (uint32_t e = lane; e < nnz_w; e += 32) bits[(__ldg(ent + e) >> 16) >> 5] = 0u;
         __syncwarp();
-        if (!LDA_CLAIM_AHEAD && lane == 0) next = (int)atomicAdd(a.tile_counter, 1u);
         tile = __shfl_sync(FULL, next, 0);
     }
     __syncwarp();
@@ -768,9 +757,6 @@ __global__ void __launch_bounds__(256, LDA_SPARSE_LARGE_MIN_BLOCKS) k_sample_spa
 }
 
 template <bool LL, int QB>
-#ifndef LDA_DENSE_DYN
-#define LDA_DENSE_DYN 1
-#endif
 __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dense_large(SampleArgs a) {
     extern __shared__ float smf[];
     __shared__ int s_tile;
@@ -848,7 +834,7 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
         double ll = sample_groups<LL, QB, false, LDA_LARGE_ROW_MODE>(a, (uint32_t)t.y, (uint32_t)t.z, 32u * wid,
                                                                      32u * warps, a.iter, maxK, ph, QL, QP, Q,
                                                                      ColShared{col}, ctr, lane, qr ? qtab : nullptr, qr,
-                                                                     nullptr, (!LL && LDA_DENSE_DYN) ? &s_group : nullptr);
+                                                                     nullptr, LL ? nullptr : &s_group);
         if (LL) {
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) ll += __shfl_xor_sync(FULL, ll, off);
