@@ -159,6 +159,13 @@ struct lda_trainer {
     // so one chunk's doc-topic rebuild and sampling overlap the other's
     cudaStream_t work[2] = {nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr, ev_join[2] = {nullptr, nullptr};
+    // above kLargeK topics a chunk's sparse-word sampler runs on a side stream of the stream
+    // that samples its dense words, so that its CTAs fill the dense kernel's tail
+    struct Side {
+        cudaStream_t parent = nullptr, stream = nullptr;
+        cudaEvent_t fork = nullptr, join = nullptr;
+    };
+    std::vector<Side> sides;
     uint32_t *h_tok_doc = nullptr, *h_dtok_pos = nullptr, *h_dtok_word = nullptr;  // pinned [N]
     std::vector<int64_t> chunk_dt;  // [C+1] first doc-row entry of each chunk
     int64_t max_chunk_tok = 0, max_chunk_dt = 0, h2d_bytes = 0;
@@ -195,6 +202,12 @@ struct lda_trainer {
             if (ev_join[i]) cudaEventDestroy(ev_join[i]);
         }
         if (ev_fork) cudaEventDestroy(ev_fork);
+        for (Side& s : sides) {
+            cudaStreamSynchronize(s.stream);
+            cudaStreamDestroy(s.stream);
+            cudaEventDestroy(s.fork);
+            cudaEventDestroy(s.join);
+        }
         cudaFreeHost(h_tok_doc);
         cudaFreeHost(h_dtok_pos);
         cudaFreeHost(h_dtok_word);
@@ -1008,6 +1021,25 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
         CUDA_TRY(cudaMemsetAsync(ad.tile_counter, 0, sizeof(unsigned), q));
         CUDA_TRY(cudaMemsetAsync(as.tile_counter, 0, sizeof(unsigned), q));
         const bool ll = ll_mode != 0;
+        // the sparse-word sampler on the side stream of q, so that its CTAs start as the
+        // dense-word kernel's CTAs run out of tiles (both read only this chunk's doc rows)
+        lda_trainer::Side* side = nullptr;
+        if (nd > 0 && ns > 0) {
+            for (auto& s : t->sides)
+                if (s.parent == q) side = &s;
+            if (!side) {
+                lda_trainer::Side s;
+                s.parent = q;
+                CUDA_TRY(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+                CUDA_TRY(cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+                CUDA_TRY(cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
+                t->sides.push_back(s);
+                side = &t->sides.back();
+            }
+            CUDA_TRY(cudaEventRecord(side->fork, q));
+            CUDA_TRY(cudaStreamWaitEvent(side->stream, side->fork, 0));
+        }
+        const cudaStream_t qs = side ? side->stream : q;
         if (nd > 0) {
             const int grid = std::max(1, std::min(t->grid_dense, nd));
             if (ll) dev::k_sample_dense_large<true, 4><<<grid, 32 * kLargeWarps, t->smem_dense, q>>>(ad);
@@ -1016,9 +1048,13 @@ static int sample_launch(lda_trainer* t, int chunk, int slot, int ll_mode, cudaS
         }
         if (ns > 0) {
             const int grid = std::max(1, std::min(t->grid_sparse, (ns + kLargeWarps - 1) / kLargeWarps));
-            if (ll) dev::k_sample_sparse_large<true, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, q>>>(as);
-            else dev::k_sample_sparse_large<false, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, q>>>(as);
+            if (ll) dev::k_sample_sparse_large<true, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, qs>>>(as);
+            else dev::k_sample_sparse_large<false, 4><<<grid, 32 * kLargeWarps, t->smem_sparse, qs>>>(as);
             CUDA_TRY(cudaGetLastError());
+        }
+        if (side) {
+            CUDA_TRY(cudaEventRecord(side->join, side->stream));
+            CUDA_TRY(cudaStreamWaitEvent(q, side->join, 0));
         }
         t->chunk_sampled_ll[chunk] = ll;
         return LDA_OK;
@@ -1172,8 +1208,12 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
     // alone nearly fill L2, and with host copies each chunk's copy waits for its sampling
     // only, so those keep one chunk per launch.
     const int cpl = (zout || t->large) ? 1 : std::max(1, (t->chunk_last - t->chunk_first + 1) / 2);
-    if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2)) {
-        // one stream, so that the stage events time each stage alone
+    if (!t->streaming && (t->timing || t->chunk_last - t->chunk_first < 2 || t->large)) {
+        // one stream, so that the stage events time each stage alone.  Resident sweeps above
+        // kLargeK topics take this path too: a chunk's doc rows (about 120 MB on the
+        // K=10,000 corpus) nearly fill L2, and a second chunk's rebuild and sampling beside
+        // them evict the rows the first chunk's sampler reads (that corpus: 131.5 -> 127.5
+        // ms per sweep on one stream).
         for (int c0 = t->chunk_first; c0 < t->chunk_last; c0 += cpl) {
             const int c1 = std::min(t->chunk_last, c0 + cpl);
             t->begin_stage(2);
