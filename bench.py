@@ -508,8 +508,10 @@ def run_ours(args, world, rank, local):
                                     "note": ("streamed: 'sample' spans copies, doc-row rebuilds and sampling "
                                              "of all chunks on their streams") if streaming else
                                             ("stages timed one at a time in a second pass over the same sweeps; "
-                                             "the timed run overlaps one chunk's doc-topic rebuild and sampling "
-                                             "with the next chunk's")},
+                                             + ("the timed run samples the chunks one after another, each chunk's "
+                                                "sparse-word sampler beside its dense-word one" if K > 2048 else
+                                                "the timed run overlaps one chunk group's doc-topic rebuild and "
+                                                "sampling with the other's"))},
             "sweep_ms_trace": trace,
             "sweep_counters": {"early_accept_frac": cnt.early_accept / max(cnt.tokens, 1),
                                "mean_nnz_full": cnt.sum_nnz_full / max(cnt.full, 1),

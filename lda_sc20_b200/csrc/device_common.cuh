@@ -336,6 +336,18 @@ struct ColSharedT {
 };
 using ColShared = ColSharedT<false>;
 
+// An L2 policy for loads of data read once per pass (evict_first), and a load with it.
+__device__ __forceinline__ uint64_t l2_stream_policy() {
+    uint64_t p;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ int ldg_hint(const int* p, uint64_t pol) {
+    int v;
+    asm("ld.global.nc.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+
 // Serial per-lane sum over the lane's entries l, l + 32, l + 64, ... of a doc row of nnz
 // entries (one fmaf chain).  A warp's loads of one step then read 32 consecutive entries,
 // one or two 128-byte lines, where contiguous per-lane blocks would touch one line per

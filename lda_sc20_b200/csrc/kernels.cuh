@@ -631,15 +631,17 @@ struct ColBits {
     const float* r;        // reciprocals in the skewed layout: r_k at col_skew(k)
     float beta;
     int maxK;
+    // Branch-free: (0 + beta) is beta exactly, so one formula gives phi_k for topics in
+    // and out of the word, and only the count's load is predicated.  The branch it replaces
+    // kept the four batched row lookups of lane_mass apart (K=10,000 corpus: samplers
+    // 115.7 -> 109.5 ms per sweep, the same topics).
     __device__ __forceinline__ float operator()(int k) const {
-        if (k == maxK) return 0.0f;
         const uint32_t b = bits[k >> 5], m = 1u << (k & 31);
         const float rk = r[col_skew(k)];
-        if (b & m) {
-            const uint32_t e = __ldg(ent + pre[k >> 5] + __popc(b & (m - 1u)));
-            return fmul(fadd(u2f(e & 0xffffu), beta), rk);
-        }
-        return fmul(beta, rk);
+        uint32_t e = 0u;
+        if (b & m) e = __ldg(ent + pre[k >> 5] + __popc(b & (m - 1u)));
+        const float phi = fmul(fadd(u2f(e & 0xffffu), beta), rk);
+        return k == maxK ? 0.0f : phi;
     }
     __device__ __forceinline__ float row(uint32_t key) const { return (*this)((int)key); }
     __device__ __forceinline__ int topic(uint32_t key) const { return (int)key; }
@@ -781,9 +783,14 @@ __global__ void __launch_bounds__(256, LDA_DENSE_LARGE_MIN_BLOCKS) k_sample_dens
         const int* wrow = a.dwt + (size_t)w * a.K;
         // phi_k = ((float)n_wk + beta) * r_k with r_k = 1 / ((float)n_k + V*beta), the values
         // fill_recip and build_column form
+        // the count row is read once per tile and chunk (800 MB per chunk on the K=10,000
+        // corpus): evict_first, so that it displaces fewer of the chunk's doc rows in L2
+        // (that corpus: samplers 116.1 -> 115.6 ms per sweep)
+        const uint64_t spol = l2_stream_policy();
         for (int k = threadIdx.x; k < a.K; k += blockDim.x) {
             const float rk = a.recip ? __ldg(a.recip + k) : __fdiv_rn(1.0f, fadd(__int2float_rn(__ldg(a.n_k + k)), a.Vbeta));
-            col[col_skew(k)] = fmul(fadd(__int2float_rn(__ldg(wrow + k)), a.beta), rk);
+            const int c = ldg_hint(wrow + k, spol);
+            col[col_skew(k)] = fmul(fadd(__int2float_rn(c), a.beta), rk);
         }
         const int maxK = (int)(__ldg(a.st_top2 + w) & 0xffffu);
         __syncthreads();
