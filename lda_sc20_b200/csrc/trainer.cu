@@ -139,6 +139,8 @@ struct lda_trainer {
     std::vector<cudaStream_t> sstreams;
     std::vector<Slot> slots;
     std::vector<cudaEvent_t> ev_slot;
+    std::vector<cudaEvent_t> ev_used;  // above kLargeK: the slot's last chunk has been sampled
+    bool stream_down = false;          // above kLargeK: the next streamed sweep takes its chunks in descending order
     cudaEvent_t ev_ready = nullptr;
     // host-buffer sweeps: each chunk's topics are copied back on copy_stream as soon as the
     // chunk is sampled
@@ -180,6 +182,7 @@ struct lda_trainer {
             cudaStreamDestroy(q);
         }
         for (cudaEvent_t e : ev_slot) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_used) cudaEventDestroy(e);
         if (ev_ready) cudaEventDestroy(ev_ready);
         if (copy_stream) {
             cudaStreamSynchronize(copy_stream);
@@ -533,9 +536,11 @@ extern "C" int lda_trainer_create(const lda_corpus* c, const lda_train_config* c
         }
         T.sstreams.resize(ns, nullptr);
         T.ev_slot.resize(ns, nullptr);
+        T.ev_used.resize(ns, nullptr);
         for (int i = 0; i < ns; ++i) {
             CUDA_TRY(cudaStreamCreateWithFlags(&T.sstreams[i], cudaStreamNonBlocking));
             CUDA_TRY(cudaEventCreateWithFlags(&T.ev_slot[i], cudaEventDisableTiming));
+            CUDA_TRY(cudaEventCreateWithFlags(&T.ev_used[i], cudaEventDisableTiming));
         }
         CUDA_TRY(cudaEventCreateWithFlags(&T.ev_ready, cudaEventDisableTiming));
         const size_t nb = sizeof(uint32_t) * (size_t)std::max<int64_t>(N, 1);
@@ -1251,6 +1256,58 @@ static int sweep_async(lda_trainer* t, int ll_mode, uint16_t* zout = nullptr, bo
             CUDA_TRY(cudaEventRecord(t->ev_join[i], t->work[i]));
             CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_join[i], 0));
         }
+    } else if (t->large) {
+        // Above kLargeK topics the chunks are rebuilt and sampled one after another on the
+        // trainer's stream (a chunk's rows nearly fill L2, as in resident sweeps).  One slot
+        // stream copies, in sampling order, each chunk that no slot holds into the slot
+        // whose chunk is needed latest (or not again in this sweep), as soon as that
+        // chunk's sampling has ended.  Sweeps alternate the chunk order, so the chunks left
+        // in the slots by one sweep are the first the next one samples, with no copy.
+        const int S = (int)t->slots.size();
+        const int n = t->chunk_last - t->chunk_first;
+        const bool down = t->stream_down;
+        auto chunk_at = [&](int i) { return down ? t->chunk_last - 1 - i : t->chunk_first + i; };
+        cudaStream_t cq = t->sstreams[0];
+        CUDA_TRY(cudaEventRecord(t->ev_ready, t->stream));
+        CUDA_TRY(cudaStreamWaitEvent(cq, t->ev_ready, 0));
+        std::vector<int> used_at(S, -1);  // order position of the slot's last sampling in this sweep
+        for (int i = 0; i < n; ++i) {
+            const int ch = chunk_at(i);
+            int slot = -1;
+            for (int k = 0; k < S; ++k)
+                if (t->slots[k].chunk == ch) slot = k;
+            if (slot < 0) {
+                // the slot whose chunk comes latest in the rest of the order (never: n),
+                // ties to the one sampled longest ago
+                int best_next = -1;
+                for (int k = 0; k < S; ++k) {
+                    const int held = t->slots[k].chunk;
+                    int next = n;
+                    if (held >= t->chunk_first && held < t->chunk_last) {
+                        const int pos = down ? t->chunk_last - 1 - held : held - t->chunk_first;
+                        if (pos > i) next = pos;
+                    }
+                    if (next > best_next || (next == best_next && used_at[k] < used_at[slot])) {
+                        best_next = next;
+                        slot = k;
+                    }
+                }
+                if (used_at[slot] >= 0) CUDA_TRY(cudaStreamWaitEvent(cq, t->ev_used[slot], 0));
+                if ((rc = load_chunk(t, ch, slot, cq))) return rc;
+                CUDA_TRY(cudaEventRecord(t->ev_slot[slot], cq));
+                CUDA_TRY(cudaStreamWaitEvent(t->stream, t->ev_slot[slot], 0));
+            }
+            t->begin_stage(2);
+            if ((rc = dt_launch(t, ch, slot, t->stream))) return rc;
+            t->end_stage();
+            t->begin_stage(3);
+            if ((rc = sample_launch(t, ch, slot, ll_mode, t->stream))) return rc;
+            t->end_stage();
+            if (zout && (rc = copy_back(t, ch, t->stream, zout))) return rc;
+            CUDA_TRY(cudaEventRecord(t->ev_used[slot], t->stream));
+            used_at[slot] = i;
+        }
+        t->stream_down = !down;
     } else {
         // chunk i of the range goes to slot / stream i mod S: its copy overlaps the
         // rebuild and sampling of the chunks on the other streams; a slot is reused in
