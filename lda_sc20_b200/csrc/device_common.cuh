@@ -352,33 +352,53 @@ __device__ __forceinline__ int ldg_hint(const int* p, uint64_t pol) {
 // entries (one fmaf chain).  A warp's loads of one step then read 32 consecutive entries,
 // one or two 128-byte lines, where contiguous per-lane blocks would touch one line per
 // lane block.
-// ROWM 1: the loads of four steps, then of two, then one, are issued before their use
-// (rows that often miss L2, at large K); ROWM 0: two steps at a time.
+// ROWM 1: the loads of four steps at a time are issued before their use (rows that often
+// miss L2, at large K); ROWM 0: two steps at a time.
 template <int ROWM = 0, class View>
 __device__ __forceinline__ float lane_mass(const typename View::Entry* __restrict__ row, uint32_t lane, uint32_t nnz,
                                            const View& colz, float acc = 0.0f) {
     using E = typename View::Entry;
-    uint32_t q = lane;
+    // Loop bounds are warp-uniform: `full` steps in which every lane has an entry, taken in
+    // batches, then the lane's last steps together with the partial step.  Bounds per lane
+    // would send the lanes of one warp through different batches, and the warp would issue
+    // each of them (K=1024 corpus: sampler 10.38 -> 9.93 ms per sweep, the same sums).
+    const uint32_t full = nnz >> 5;
+    const E* __restrict__ p = row + lane;
+    uint32_t s = 0;
     if (ROWM == 1) {
-        for (; q + 96u < nnz; q += 128u) {
-        const E e0 = __ldg(row + q), e1 = __ldg(row + q + 32u), e2 = __ldg(row + q + 64u),
-                e3 = __ldg(row + q + 96u);
-        acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
-        acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
-        acc = ffma(colz.cnt(e2), colz.row(colz.key(e2)), acc);
-        acc = ffma(colz.cnt(e3), colz.row(colz.key(e3)), acc);
+        for (; s + 4u <= full; s += 4u) {
+            const E e0 = __ldg(p + 32u * s), e1 = __ldg(p + 32u * s + 32u), e2 = __ldg(p + 32u * s + 64u),
+                    e3 = __ldg(p + 32u * s + 96u);
+            acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
+            acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
+            acc = ffma(colz.cnt(e2), colz.row(colz.key(e2)), acc);
+            acc = ffma(colz.cnt(e3), colz.row(colz.key(e3)), acc);
         }
+        // the lane's last steps (up to three full ones and the partial one): their loads
+        // issued together, so that a row of up to 256 entries costs two rounds of loads
+        const uint32_t nl = full + (lane < (nnz & 31u) ? 1u : 0u);
+        if (s < full + ((nnz & 31u) ? 1u : 0u)) {
+            E e[4];
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; ++j) e[j] = s + j < nl ? __ldg(p + 32u * (s + j)) : E{};
+#pragma unroll
+            for (uint32_t j = 0; j < 4u; ++j)
+                if (s + j < nl) acc = ffma(colz.cnt(e[j]), colz.row(colz.key(e[j])), acc);
+        }
+        return acc;
     }
-    // the loads of two steps issued together
-    for (; q + 32u < nnz; q += 64u) {
-        const E e0 = __ldg(row + q), e1 = __ldg(row + q + 32u);
+    for (; s + 2u <= full; s += 2u) {
+        const E e0 = __ldg(p + 32u * s), e1 = __ldg(p + 32u * s + 32u);
         acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
         acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
     }
-    if (q < nnz) {
-        const E e = __ldg(row + q);
-        acc = ffma(colz.cnt(e), colz.row(colz.key(e)), acc);
-    }
+    // the last full step (if any) and the lanes of the partial step, loads issued together
+    const bool one = s < full, tail = lane < (nnz & 31u);
+    E e0{}, e1{};
+    if (one) e0 = __ldg(p + 32u * s);
+    if (tail) e1 = __ldg(p + 32u * full);
+    if (one) acc = ffma(colz.cnt(e0), colz.row(colz.key(e0)), acc);
+    if (tail) acc = ffma(colz.cnt(e1), colz.row(colz.key(e1)), acc);
     return acc;
 }
 
