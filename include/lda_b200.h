@@ -131,7 +131,9 @@ typedef struct {
     int64_t device_budget;  /* bytes the trainer may allocate (0: no limit) */
     int32_t stream_mode;    /* 0: keep the corpus resident when it fits device_budget, else
                                stream it; 1: always resident; 2: always stream */
-    int32_t num_streams;    /* streaming: CUDA streams = chunk slots on the device (0: 4) */
+    int32_t num_streams;    /* streaming: chunk slots on the device, one CUDA stream each (0: 4);
+                               above 2048 topics the chunks are sampled in turn and a slot
+                               keeps its chunk across sweeps */
     int32_t num_dense;      /* 0: the corpus' dense/sparse split; n > 0: words [0, n) use the
                                dense word-topic path; -1: none (results do not depend on it) */
 } lda_train_config;
