@@ -225,7 +225,7 @@ def run_sharded(args, world, rank, local):
     corpus = make_corpus(args.preset, 0, args.chunks)
     info = corpus.info
     K, N = info.K_hint, info.num_tokens
-    st = ShardedTrainer(corpus, K=K, rank=rank, world=world, device=local, seed=42)
+    st = ShardedTrainer(corpus, K=K, rank=rank, world=world, device=local, seed=42, alpha=ALPHA.get(args.preset))
     stream = torch.cuda.current_stream()
     z0 = corpus.topics()
     seg = corpus.seg_cnt()
@@ -240,8 +240,6 @@ def run_sharded(args, world, rank, local):
     st.iterate(args.warmup)
     st.tr.set_topics(z0)
     st.tr.iteration = 0
-    st.tr.reset_stats()
-    st.tr.set_timing(True)
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -252,14 +250,22 @@ def run_sharded(args, world, rank, local):
     dist.barrier()
     clk = clocks.stop()
     ms = reduce_max(e0.elapsed_time(e1))
-    tm = st.tr.timing()
-    cnt = st.tr.counters()
-    st.tr.set_timing(False)
     z_after = st.topics()
     h = torch.tensor([int(z_after[::101].astype(np.int64).sum())], dtype=torch.int64, device="cuda")
     hs = [torch.zeros_like(h) for _ in range(world)]
     dist.all_gather(hs, h)
     agree = all(int(x.item()) == int(h.item()) for x in hs)
+    # the same sweeps again with per-stage CUDA events (stages one at a time on the
+    # trainer's stream), for the stage split and the sampler's roofline
+    st.tr.set_topics(z0)
+    st.tr.iteration = 0
+    st.tr.reset_stats()
+    st.tr.set_timing(True)
+    st.iterate(args.steps)
+    torch.cuda.synchronize()
+    tm = st.tr.timing()
+    cnt = st.tr.counters()
+    st.tr.set_timing(False)
     ll_mean = st.iterate(1, ll=True)
     # end to end: each rank uploads its chunks' topics, exchanges, sweeps, downloads its chunks
     e2e = None
